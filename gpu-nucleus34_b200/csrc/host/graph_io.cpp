@@ -1,0 +1,346 @@
+// Host graph layer: readers (.mtx/.edges/.txt/.grh), undirected CSR build,
+// degree orientation and the .grh writer, with the reference's semantics:
+//   from_edges      nucleus/graph/graph.hpp:285-411
+//   make_oriented   nucleus/graph/graph.hpp:176-218 (vertex_less, graph_api.hpp:124-127)
+//   deserialize     nucleus/graph/graph.hpp:491-520, build_offset :523-536
+//   serialize       nucleus/graph/graph.hpp:465-488
+// The parse is parallel (OpenMP over line-aligned chunks) and the pair
+// sort + unique of from_edges is done as a counting sort by source followed by
+// a per-list sort + unique, which yields the same sorted unique adjacency.
+#include "host_internal.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cerrno>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <omp.h>
+
+namespace n34 {
+
+namespace {
+
+bool is_digit(char c) { return c >= '0' && c <= '9'; }
+
+// "<uint> <uint>" at the start of a line, as `ss >> s >> d` reads well-formed
+// input (graph.hpp:361-363). Lines without two numbers are skipped (the
+// reference reads uninitialised values for them).
+inline bool parse_two(const char *p, const char *end, uint32_t &s, uint32_t &d)
+{
+	while (p < end && (*p == ' ' || *p == '\t'))
+		++p;
+	if (p >= end || !is_digit(*p))
+		return false;
+	uint64_t a = 0;
+	while (p < end && is_digit(*p))
+	{
+		a = a * 10 + uint64_t(*p - '0');
+		if (a > 0xffffffffull)
+			return false;
+		++p;
+	}
+	while (p < end && (*p == ' ' || *p == '\t'))
+		++p;
+	if (p >= end || !is_digit(*p))
+		return false;
+	uint64_t b = 0;
+	while (p < end && is_digit(*p))
+	{
+		b = b * 10 + uint64_t(*p - '0');
+		if (b > 0xffffffffull)
+			return false;
+		++p;
+	}
+	s = uint32_t(a);
+	d = uint32_t(b);
+	return true;
+}
+
+std::string file_ext(const std::string &path)
+{
+	auto dot = path.find_last_of('.');
+	auto slash = path.find_last_of('/');
+	if (dot == std::string::npos || (slash != std::string::npos && dot < slash))
+		return "";
+	return path.substr(dot);
+}
+
+int read_file(const char *path, std::vector<char> &buf)
+{
+	FILE *f = std::fopen(path, "rb");
+	if (!f)
+		return fail(NUCLEUS34_E_IO, std::string("Dataset ") + path + " is not accessible!");
+	std::fseek(f, 0, SEEK_END);
+	long sz = std::ftell(f);
+	std::fseek(f, 0, SEEK_SET);
+	if (sz < 0)
+	{
+		std::fclose(f);
+		return fail(NUCLEUS34_E_IO, "cannot size file");
+	}
+	buf.resize(size_t(sz) + 1);
+	size_t got = sz ? std::fread(buf.data(), 1, size_t(sz), f) : 0;
+	std::fclose(f);
+	if (got != size_t(sz))
+		return fail(NUCLEUS34_E_IO, "short read");
+	buf[size_t(sz)] = '\n';
+	buf.resize(size_t(sz));
+	return NUCLEUS34_OK;
+}
+
+} // namespace
+
+int build_oriented(const uint32_t *src, const uint32_t *dst, uint64_t count, HostGraph &out)
+{
+	// max_node over non-self-loop pairs only (graph.hpp:365-369)
+	uint32_t max_node = 0;
+#pragma omp parallel for reduction(max : max_node) schedule(static)
+	for (int64_t i = 0; i < int64_t(count); ++i)
+		if (src[i] != dst[i])
+			max_node = std::max(max_node, std::max(src[i], dst[i]));
+	const uint64_t n = uint64_t(max_node) + 1;
+
+	// undirected CSR by counting sort on the source, both directions
+	std::vector<uint64_t> off(n + 1, 0);
+	{
+		std::vector<std::atomic<uint32_t>> deg(n);
+#pragma omp parallel for schedule(static)
+		for (int64_t v = 0; v < int64_t(n); ++v)
+			deg[v].store(0, std::memory_order_relaxed);
+#pragma omp parallel for schedule(static)
+		for (int64_t i = 0; i < int64_t(count); ++i)
+			if (src[i] != dst[i])
+			{
+				deg[src[i]].fetch_add(1, std::memory_order_relaxed);
+				deg[dst[i]].fetch_add(1, std::memory_order_relaxed);
+			}
+		for (uint64_t v = 0; v < n; ++v)
+			off[v + 1] = off[v] + deg[v].load(std::memory_order_relaxed);
+	}
+	const uint64_t total = off[n];
+	std::vector<uint32_t> adj(total ? total : 1);
+	{
+		std::vector<std::atomic<uint64_t>> cur(n);
+#pragma omp parallel for schedule(static)
+		for (int64_t v = 0; v < int64_t(n); ++v)
+			cur[v].store(off[v], std::memory_order_relaxed);
+#pragma omp parallel for schedule(static)
+		for (int64_t i = 0; i < int64_t(count); ++i)
+			if (src[i] != dst[i])
+			{
+				adj[cur[src[i]].fetch_add(1, std::memory_order_relaxed)] = dst[i];
+				adj[cur[dst[i]].fetch_add(1, std::memory_order_relaxed)] = src[i];
+			}
+	}
+	// per-list sort + unique == global pair sort + unique (graph.hpp:383-388)
+	std::vector<uint32_t> udeg(n, 0);
+#pragma omp parallel for schedule(dynamic, 256)
+	for (int64_t v = 0; v < int64_t(n); ++v)
+	{
+		uint32_t *b = adj.data() + off[v], *e = adj.data() + off[v + 1];
+		std::sort(b, e);
+		udeg[v] = uint32_t(std::unique(b, e) - b);
+	}
+	// orientation on the undirected degree (graph.hpp:196-213)
+	out.n = n;
+	out.O.assign(n + 1, 0);
+	out.D.assign(n, 0);
+#pragma omp parallel for schedule(dynamic, 256)
+	for (int64_t u = 0; u < int64_t(n); ++u)
+	{
+		uint32_t k = 0;
+		const uint32_t du = udeg[u];
+		for (uint64_t j = off[u]; j < off[u] + udeg[u]; ++j)
+		{
+			const uint32_t v = adj[j];
+			if (du < udeg[v] || (du == udeg[v] && uint32_t(u) < v))
+				++k;
+		}
+		out.D[u] = k;
+	}
+	for (uint64_t u = 0; u < n; ++u)
+	{
+		if (uint64_t(out.O[u]) + out.D[u] > 0xffffffffull)
+			return fail(NUCLEUS34_E_RANGE32, "oriented edge count exceeds 32-bit edge ids");
+		out.O[u + 1] = out.O[u] + out.D[u];
+	}
+	out.m = out.O[n];
+	out.E.assign(out.m ? out.m : 1, 0);
+	out.E.resize(out.m);
+#pragma omp parallel for schedule(dynamic, 256)
+	for (int64_t u = 0; u < int64_t(n); ++u)
+	{
+		uint32_t w = out.O[u];
+		const uint32_t du = udeg[u];
+		for (uint64_t j = off[u]; j < off[u] + udeg[u]; ++j)
+		{
+			const uint32_t v = adj[j];
+			if (du < udeg[v] || (du == udeg[v] && uint32_t(u) < v))
+				out.E[w++] = v;
+		}
+	}
+	return NUCLEUS34_OK;
+}
+
+int load_graph(const char *path, HostGraph &g)
+{
+	if (!path)
+		return fail(NUCLEUS34_E_INVALID, "null path");
+	const std::string ext = file_ext(path);
+	if (ext == ".grh")
+	{
+		FILE *f = std::fopen(path, "rb");
+		if (!f)
+			return fail(NUCLEUS34_E_IO, "Can't open file for reading.");
+		uint64_t sv = 0, nV = 0, nE = 0;
+		bool ok = std::fread(&sv, 8, 1, f) == 1 && std::fread(&nV, 8, 1, f) == 1 &&
+				  std::fread(&nE, 8, 1, f) == 1;
+		if (!ok || sv != sizeof(uint32_t))
+		{
+			std::fclose(f);
+			return fail(NUCLEUS34_E_FORMAT, "Incompatible types in dataset.");
+		}
+		if (nE > 0xffffffffull)
+		{
+			std::fclose(f);
+			return fail(NUCLEUS34_E_RANGE32, "edge count exceeds 32-bit edge ids");
+		}
+		g.n = nV;
+		g.D.resize(nV);
+		g.E.resize(nE);
+		ok = (nV == 0 || std::fread(g.D.data(), 4, nV, f) == nV) &&
+			 (nE == 0 || std::fread(g.E.data(), 4, nE, f) == nE);
+		std::fclose(f);
+		if (!ok)
+			return fail(NUCLEUS34_E_FORMAT, "truncated .grh file");
+		g.O.assign(nV + 1, 0);
+		for (uint64_t u = 0; u < nV; ++u)
+			g.O[u + 1] = g.O[u] + g.D[u];
+		if (g.O[nV] != nE)
+			return fail(NUCLEUS34_E_FORMAT, ".grh degree sum does not match its edge count");
+		g.m = nE;
+		return NUCLEUS34_OK;
+	}
+	const bool mtx = ext == ".mtx";
+	if (!mtx && ext != ".edges" && ext != ".txt")
+		return fail(NUCLEUS34_E_FORMAT, "Unknown dataset format: " + ext);
+
+	std::vector<char> buf;
+	int rc = read_file(path, buf);
+	if (rc)
+		return rc;
+	const char *p = buf.data(), *end = buf.data() + buf.size();
+
+	// Skip leading comment lines: a line whose first character is '#' or '%'
+	// (graph.hpp:307-314). The first other line is the header: parsed for
+	// .mtx, consumed and discarded for bare edge lists (graph.hpp:318-359).
+	const char *line = p;
+	const char *header = nullptr, *header_end = nullptr;
+	while (line < end)
+	{
+		const char *nl = static_cast<const char *>(std::memchr(line, '\n', size_t(end - line)));
+		const char *le = nl ? nl : end;
+		const char *next = nl ? nl + 1 : end;
+		if (le == line || (*line != '#' && *line != '%'))
+		{
+			header = line;
+			header_end = le;
+			line = next;
+			break;
+		}
+		line = next;
+	}
+	if (mtx)
+	{
+		if (!header)
+			return fail(NUCLEUS34_E_FORMAT, "Wrong header for mtx format!");
+		std::vector<unsigned long long> tok;
+		std::string h(header, header_end);
+		char *save = nullptr;
+		for (char *t = strtok_r(h.data(), " \t\r", &save); t; t = strtok_r(nullptr, " \t\r", &save))
+		{
+			char *e2 = nullptr;
+			errno = 0;
+			unsigned long long v = std::strtoull(t, &e2, 0);
+			if (e2 == t || errno)
+				return fail(NUCLEUS34_E_FORMAT, "Wrong header for mtx format!");
+			tok.push_back(v);
+		}
+		if (tok.size() != 2 && tok.size() != 3)
+			return fail(NUCLEUS34_E_FORMAT, "Wrong header for mtx format!");
+		unsigned long long nv = tok.size() == 2 ? tok[0] : std::max(tok[0], tok[1]);
+		unsigned long long ne = tok.size() == 2 ? tok[1] : tok[2];
+		if (ne > 0xffffffffull)
+			return fail(NUCLEUS34_E_RANGE32, "Edges size are larger than defined type.");
+		if (nv > 0xffffffffull)
+			return fail(NUCLEUS34_E_RANGE32, "Vertices id are larger than defined type.");
+	}
+	if (!header)
+		line = end; // nothing but comments
+
+	// parallel parse of the remaining lines
+	const size_t body = size_t(end - line);
+	const int nth = std::max(1, omp_get_max_threads());
+	const int nchunks = body < (1u << 20) ? 1 : nth * 4;
+	std::vector<const char *> cb(nchunks + 1);
+	cb[0] = line;
+	cb[nchunks] = end;
+	for (int c = 1; c < nchunks; ++c)
+	{
+		const char *q = line + body * size_t(c) / size_t(nchunks);
+		if (q < cb[c - 1])
+			q = cb[c - 1];
+		const char *nl = static_cast<const char *>(std::memchr(q, '\n', size_t(end - q)));
+		cb[c] = nl ? nl + 1 : end;
+	}
+	std::vector<std::vector<uint32_t>> ps(nchunks), pd(nchunks);
+#pragma omp parallel for schedule(dynamic, 1)
+	for (int c = 0; c < nchunks; ++c)
+	{
+		const char *q = cb[c], *qe = cb[c + 1];
+		auto &S = ps[c];
+		auto &Dd = pd[c];
+		while (q < qe)
+		{
+			const char *nl = static_cast<const char *>(std::memchr(q, '\n', size_t(qe - q)));
+			const char *le = nl ? nl : qe;
+			uint32_t s, d;
+			if (parse_two(q, le, s, d))
+			{
+				S.push_back(s);
+				Dd.push_back(d);
+			}
+			q = nl ? nl + 1 : qe;
+		}
+	}
+	std::vector<uint64_t> coff(nchunks + 1, 0);
+	for (int c = 0; c < nchunks; ++c)
+		coff[c + 1] = coff[c] + ps[c].size();
+	std::vector<uint32_t> S(coff[nchunks]), Dd(coff[nchunks]);
+#pragma omp parallel for schedule(dynamic, 1)
+	for (int c = 0; c < nchunks; ++c)
+	{
+		std::copy(ps[c].begin(), ps[c].end(), S.begin() + coff[c]);
+		std::copy(pd[c].begin(), pd[c].end(), Dd.begin() + coff[c]);
+	}
+	return build_oriented(S.data(), Dd.data(), S.size(), g);
+}
+
+int save_grh(const nucleus34_graph *g, const char *path)
+{
+	FILE *f = std::fopen(path, "wb");
+	if (!f)
+		return fail(NUCLEUS34_E_IO, "Can't open file for serializing.");
+	uint64_t hdr[3] = {sizeof(uint32_t), g->n, g->m};
+	bool ok = std::fwrite(hdr, 8, 3, f) == 3 &&
+			  (g->n == 0 || std::fwrite(g->D, 4, g->n, f) == g->n) &&
+			  (g->m == 0 || std::fwrite(g->E, 4, g->m, f) == g->m);
+	ok = (std::fclose(f) == 0) && ok;
+	return ok ? NUCLEUS34_OK : fail(NUCLEUS34_E_IO, "short write");
+}
+
+} // namespace n34

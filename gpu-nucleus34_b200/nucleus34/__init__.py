@@ -1,0 +1,352 @@
+"""ctypes binding of libnucleus34 (the C-ABI declared in include/nucleus34.h).
+
+This is the Python face of the library for the tests, the bench and
+scripting: every call goes through the same extern "C" entry points a C/C++
+caller uses. The library must be built first (``make -C gpu-nucleus34_b200``);
+there is no pure-Python or CPU fallback for the decomposition -- a missing
+library raises.
+
+Reference mapping: ``decompose(..., variant="direct")`` is the device
+pipeline of nucleus/cuNucleus34.cu:283-721, ``variant="ondemand"`` that of
+nucleus/cuNucleus34_ondemand.cu:407-690; ``load_graph`` is graph_t::from_edges
+/ deserialize + make_oriented (nucleus/graph/graph.hpp:176-218, 285-411,
+491-536).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+ROOT_DIR = os.path.dirname(PKG_DIR)
+LIB_PATH = os.path.join(ROOT_DIR, "lib", "libnucleus34.so")
+BIN_DIR = os.path.join(ROOT_DIR, "bin")
+
+OK = 0
+E_INVALID = -1
+E_OOM_BUDGET = -2
+E_RANGE32 = -3
+E_CUDA = -4
+E_TIMEOUT = -5
+E_IO = -6
+E_FORMAT = -7
+E_NODEVICE = -8
+E_STATE = -9
+
+DIRECT = 0
+ONDEMAND = 1
+_VARIANTS = {"direct": DIRECT, "ondemand": ONDEMAND, DIRECT: DIRECT, ONDEMAND: ONDEMAND}
+
+# Every symbol include/nucleus34.h declares (checked by the CPU test suite).
+EXPORTED = (
+    "nucleus34_decompose", "nucleus34_decompose_ondemand", "nucleus34_copy_k",
+    "nucleus34_copy_quds", "nucleus34_write_kfile", "nucleus34_free",
+    "nucleus34_strerror", "nucleus34_last_error",
+    "nucleus34_ctx_create", "nucleus34_ctx_upload", "nucleus34_ctx_run",
+    "nucleus34_ctx_copy_k", "nucleus34_ctx_destroy",
+    "nucleus34_graph_load", "nucleus34_graph_from_edges", "nucleus34_graph_save_grh",
+    "nucleus34_graph_release", "nucleus34_graph_csr",
+    "nucleus34_gen_rmat", "nucleus34_gen_rgg", "nucleus34_gen_ws",
+    "nucleus34_edges_write", "nucleus34_edges_release", "nucleus34_splitmix64",
+)
+
+
+class Nucleus34Error(RuntimeError):
+    def __init__(self, code: int, where: str, detail: str = ""):
+        self.code = code
+        msg = f"{where}: {strerror(code)} ({code})"
+        if detail:
+            msg += f": {detail}"
+        super().__init__(msg)
+
+
+class Csr(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("m", C.c_uint64), ("O", C.POINTER(C.c_uint32)),
+                ("D", C.POINTER(C.c_uint32)), ("E", C.POINTER(C.c_uint32))]
+
+
+class Opts(C.Structure):
+    _fields_ = [("mem_budget_bytes", C.c_uint64), ("device", C.c_int),
+                ("parts", C.c_uint32), ("tune_table", C.c_char_p)]
+
+
+class Result(C.Structure):
+    _fields_ = [("triangle_count", C.c_uint64), ("four_clique_count", C.c_uint64),
+                ("peeling_iterations", C.c_uint64), ("unpeeled_count", C.c_uint64),
+                ("k_max", C.c_uint32), ("k_avg", C.c_double),
+                ("t_triangles", C.c_double), ("t_incidence", C.c_double),
+                ("t_support", C.c_double), ("t_cliques", C.c_double),
+                ("t_peel", C.c_double), ("t_total", C.c_double),
+                ("incidence_entries", C.c_uint64), ("gpu_launches", C.c_uint64),
+                ("peak_device_bytes", C.c_uint64), ("variant", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Graph(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("m", C.c_uint64), ("O", C.POINTER(C.c_uint32)),
+                ("D", C.POINTER(C.c_uint32)), ("E", C.POINTER(C.c_uint32))]
+
+
+class Edges(C.Structure):
+    _fields_ = [("count", C.c_uint64), ("src", C.POINTER(C.c_uint32)),
+                ("dst", C.POINTER(C.c_uint32))]
+
+
+_LIB: Optional[C.CDLL] = None
+
+
+def lib() -> C.CDLL:
+    """Loads libnucleus34.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(
+            f"{LIB_PATH} is missing: build it with `make -C {ROOT_DIR}` "
+            "(there is no fallback implementation)")
+    L = C.CDLL(LIB_PATH)
+    u32p, u64 = C.POINTER(C.c_uint32), C.c_uint64
+    L.nucleus34_strerror.restype = C.c_char_p
+    L.nucleus34_strerror.argtypes = [C.c_int]
+    L.nucleus34_last_error.restype = C.c_char_p
+    L.nucleus34_last_error.argtypes = []
+    for fn in ("nucleus34_decompose", "nucleus34_decompose_ondemand"):
+        getattr(L, fn).argtypes = [C.POINTER(Csr), C.POINTER(Opts), C.POINTER(Result), C.POINTER(C.c_void_p)]
+        getattr(L, fn).restype = C.c_int
+    L.nucleus34_copy_k.argtypes = [C.c_void_p, C.POINTER(C.c_int32), u32p]
+    L.nucleus34_copy_k.restype = C.c_int
+    L.nucleus34_copy_quds.argtypes = [C.c_void_p, u64, u64, u32p]
+    L.nucleus34_copy_quds.restype = C.c_int
+    L.nucleus34_write_kfile.argtypes = [C.c_void_p, C.c_char_p]
+    L.nucleus34_write_kfile.restype = C.c_int
+    L.nucleus34_free.argtypes = [C.c_void_p]
+    L.nucleus34_free.restype = None
+    L.nucleus34_ctx_create.argtypes = [C.POINTER(Opts), C.POINTER(C.c_void_p)]
+    L.nucleus34_ctx_create.restype = C.c_int
+    L.nucleus34_ctx_upload.argtypes = [C.c_void_p, C.POINTER(Csr)]
+    L.nucleus34_ctx_upload.restype = C.c_int
+    L.nucleus34_ctx_run.argtypes = [C.c_void_p, C.c_int, C.POINTER(Result)]
+    L.nucleus34_ctx_run.restype = C.c_int
+    L.nucleus34_ctx_copy_k.argtypes = [C.c_void_p, C.POINTER(C.c_int32), u32p]
+    L.nucleus34_ctx_copy_k.restype = C.c_int
+    L.nucleus34_ctx_destroy.argtypes = [C.c_void_p]
+    L.nucleus34_ctx_destroy.restype = None
+    L.nucleus34_graph_load.argtypes = [C.c_char_p, C.POINTER(Graph)]
+    L.nucleus34_graph_load.restype = C.c_int
+    L.nucleus34_graph_from_edges.argtypes = [u32p, u32p, u64, C.POINTER(Graph)]
+    L.nucleus34_graph_from_edges.restype = C.c_int
+    L.nucleus34_graph_save_grh.argtypes = [C.POINTER(Graph), C.c_char_p]
+    L.nucleus34_graph_save_grh.restype = C.c_int
+    L.nucleus34_graph_release.argtypes = [C.POINTER(Graph)]
+    L.nucleus34_graph_release.restype = None
+    L.nucleus34_gen_rmat.argtypes = [C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double, u64, C.POINTER(Edges)]
+    L.nucleus34_gen_rmat.restype = C.c_int
+    L.nucleus34_gen_rgg.argtypes = [u64, C.c_double, u64, C.POINTER(Edges)]
+    L.nucleus34_gen_rgg.restype = C.c_int
+    L.nucleus34_gen_ws.argtypes = [u64, C.c_uint32, C.c_double, u64, C.POINTER(Edges)]
+    L.nucleus34_gen_ws.restype = C.c_int
+    L.nucleus34_edges_write.argtypes = [C.POINTER(Edges), C.c_char_p]
+    L.nucleus34_edges_write.restype = C.c_int
+    L.nucleus34_edges_release.argtypes = [C.POINTER(Edges)]
+    L.nucleus34_edges_release.restype = None
+    L.nucleus34_splitmix64.argtypes = [u64]
+    L.nucleus34_splitmix64.restype = u64
+    _LIB = L
+    return L
+
+
+def strerror(code: int) -> str:
+    return lib().nucleus34_strerror(code).decode()
+
+
+def last_error() -> str:
+    return lib().nucleus34_last_error().decode()
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != OK:
+        raise Nucleus34Error(rc, where, last_error())
+
+
+def _u32p(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def splitmix64(x: int) -> int:
+    return int(lib().nucleus34_splitmix64(C.c_uint64(x & 0xFFFFFFFFFFFFFFFF)))
+
+
+# ---------------------------------------------------------------- graphs ----
+
+@dataclass
+class HostGraph:
+    """Oriented CSR as numpy arrays (O has n+1 entries)."""
+    n: int
+    m: int
+    O: np.ndarray
+    D: np.ndarray
+    E: np.ndarray
+
+    def csr(self) -> Csr:
+        return Csr(self.n, self.m, _u32p(self.O), _u32p(self.D), _u32p(self.E))
+
+
+def _take_graph(g: Graph) -> HostGraph:
+    L = lib()
+    n, m = int(g.n), int(g.m)
+    O = np.ctypeslib.as_array(g.O, shape=(n + 1,)).copy()
+    D = np.ctypeslib.as_array(g.D, shape=(n,)).copy() if n else np.zeros(0, np.uint32)
+    E = np.ctypeslib.as_array(g.E, shape=(m,)).copy() if m else np.zeros(0, np.uint32)
+    L.nucleus34_graph_release(C.byref(g))
+    return HostGraph(n, m, O, D, E)
+
+
+def load_graph(path: str) -> HostGraph:
+    g = Graph()
+    _check(lib().nucleus34_graph_load(os.fsencode(path), C.byref(g)), f"load_graph({path})")
+    return _take_graph(g)
+
+
+def graph_from_edges(src: np.ndarray, dst: np.ndarray) -> HostGraph:
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    g = Graph()
+    _check(lib().nucleus34_graph_from_edges(_u32p(src), _u32p(dst), len(src), C.byref(g)),
+           "graph_from_edges")
+    return _take_graph(g)
+
+
+def save_grh(g: HostGraph, path: str) -> None:
+    gg = Graph(g.n, g.m, _u32p(g.O), _u32p(g.D), _u32p(g.E))
+    _check(lib().nucleus34_graph_save_grh(C.byref(gg), os.fsencode(path)), "save_grh")
+
+
+# ------------------------------------------------------------ generators ----
+
+def _take_edges(e: Edges):
+    c = int(e.count)
+    src = np.ctypeslib.as_array(e.src, shape=(c,)).copy() if c else np.zeros(0, np.uint32)
+    dst = np.ctypeslib.as_array(e.dst, shape=(c,)).copy() if c else np.zeros(0, np.uint32)
+    lib().nucleus34_edges_release(C.byref(e))
+    return src, dst
+
+
+def gen_rmat(scale: int, edge_factor: int, seed: int, a=0.57, b=0.19, c=0.19):
+    e = Edges()
+    _check(lib().nucleus34_gen_rmat(scale, edge_factor, a, b, c, seed, C.byref(e)), "gen_rmat")
+    return _take_edges(e)
+
+
+def gen_rgg(n: int, degree: float, seed: int):
+    e = Edges()
+    _check(lib().nucleus34_gen_rgg(n, degree, seed, C.byref(e)), "gen_rgg")
+    return _take_edges(e)
+
+
+def gen_ws(n: int, k: int, beta: float, seed: int):
+    e = Edges()
+    _check(lib().nucleus34_gen_ws(n, k, beta, seed, C.byref(e)), "gen_ws")
+    return _take_edges(e)
+
+
+def write_edges(src: np.ndarray, dst: np.ndarray, path: str) -> None:
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    e = Edges(len(src), _u32p(src), _u32p(dst))
+    _check(lib().nucleus34_edges_write(C.byref(e), os.fsencode(path)), "write_edges")
+
+
+# --------------------------------------------------------- decomposition ----
+
+@dataclass
+class Decomposition:
+    result: dict
+    k: np.ndarray
+    tris: np.ndarray
+    quds: Optional[np.ndarray] = None
+    extra: dict = field(default_factory=dict)
+
+
+def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1) -> Opts:
+    return Opts(mem_budget_bytes, device, parts, None)
+
+
+def decompose(g: HostGraph, variant="direct", device: int = 0, mem_budget_bytes: int = 0,
+              n_quds: int = 5, kfile: Optional[str] = None) -> Decomposition:
+    """One-shot decomposition through nucleus34_decompose[_ondemand]."""
+    L = lib()
+    v = _VARIANTS[variant]
+    opts = make_opts(device, mem_budget_bytes)
+    res = Result()
+    h = C.c_void_p()
+    csr = g.csr()
+    fn = L.nucleus34_decompose if v == DIRECT else L.nucleus34_decompose_ondemand
+    _check(fn(C.byref(csr), C.byref(opts), C.byref(res), C.byref(h)), "decompose")
+    try:
+        T = int(res.triangle_count)
+        k = np.zeros(T, np.int32)
+        tris = np.zeros(3 * T, np.uint32)
+        _check(L.nucleus34_copy_k(h, k.ctypes.data_as(C.POINTER(C.c_int32)), _u32p(tris)), "copy_k")
+        quds = None
+        if v == DIRECT and n_quds:
+            q = min(int(n_quds), int(res.four_clique_count))
+            quds = np.zeros(4 * q, np.uint32)
+            if q:
+                _check(L.nucleus34_copy_quds(h, 0, q, _u32p(quds)), "copy_quds")
+            quds = quds.reshape(-1, 4)
+        if kfile:
+            _check(L.nucleus34_write_kfile(h, os.fsencode(kfile)), "write_kfile")
+        return Decomposition(res.as_dict(), k, tris.reshape(-1, 3), quds)
+    finally:
+        L.nucleus34_free(h)
+
+
+class Context:
+    """Device-resident context: upload once, run many times."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0):
+        self._L = lib()
+        self._opts = make_opts(device, mem_budget_bytes)
+        self._h = C.c_void_p()
+        _check(self._L.nucleus34_ctx_create(C.byref(self._opts), C.byref(self._h)), "ctx_create")
+
+    def upload(self, g: HostGraph) -> None:
+        csr = g.csr()
+        _check(self._L.nucleus34_ctx_upload(self._h, C.byref(csr)), "ctx_upload")
+
+    def run(self, variant="ondemand") -> dict:
+        res = Result()
+        _check(self._L.nucleus34_ctx_run(self._h, _VARIANTS[variant], C.byref(res)), "ctx_run")
+        self._last = res.as_dict()
+        return self._last
+
+    def copy_k(self, T: int, with_tris: bool = False):
+        k = np.zeros(T, np.int32)
+        tris = np.zeros(3 * T, np.uint32) if with_tris else None
+        _check(self._L.nucleus34_ctx_copy_k(
+            self._h, k.ctypes.data_as(C.POINTER(C.c_int32)),
+            _u32p(tris) if tris is not None else None), "ctx_copy_k")
+        return (k, tris.reshape(-1, 3)) if with_tris else k
+
+    def close(self) -> None:
+        if self._h:
+            self._L.nucleus34_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

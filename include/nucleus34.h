@@ -1,0 +1,197 @@
+/*
+ * nucleus34.h -- C-ABI of the B200-native (3,4)-nucleus decomposition.
+ *
+ * Plain pointers and sizes only; no exception crosses this boundary and every
+ * entry point returns a status code (0 = success, negative = NUCLEUS34_E_*).
+ *
+ * Vertex and edge ids are uint32, exactly as the reference's CSR holds them
+ * (graph_t<EDGE_T=unsigned, VERTEX_T=unsigned>, nucleus/graph/graph_api.hpp:17-52):
+ * an oriented edge id is its position in the degree-oriented CSR whose
+ * adjacency lists are in ascending vertex-id order. A triangle is the triple
+ * (a,b,c) of oriented-edge ids (u,w),(u,v),(v,w) (tri_t, nucleus/utils.cuh:93-102);
+ * triangle ids are positions in the canonical (a,b) order.
+ *
+ * Threading: each call is synchronous on a library-owned stream of
+ * opts->device. Calls on distinct handles/contexts may run concurrently from
+ * different host threads.
+ */
+#ifndef NUCLEUS34_H_
+#define NUCLEUS34_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NUCLEUS34_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+enum
+{
+	NUCLEUS34_OK = 0,
+	NUCLEUS34_E_INVALID = -1,     /* bad argument or malformed CSR */
+	NUCLEUS34_E_OOM_BUDGET = -2,  /* device memory budget exceeded (reference: bad_alloc /
+	                                 segment retry exhausted, nucleus/utils.cuh:1580-1581) */
+	NUCLEUS34_E_RANGE32 = -3,     /* a 32-bit id range would overflow (reference guards:
+	                                 nucleus/cuNucleus34.cu:617-624, cuNucleus34_ondemand.cu:505-511) */
+	NUCLEUS34_E_CUDA = -4,        /* CUDA runtime error */
+	NUCLEUS34_E_TIMEOUT = -5,     /* a bounded device wait ran out */
+	NUCLEUS34_E_IO = -6,          /* file could not be opened/read/written */
+	NUCLEUS34_E_FORMAT = -7,      /* unknown extension or malformed file
+	                                 (reference: "Unknown dataset format", cuNucleus34.cu:253-256) */
+	NUCLEUS34_E_NODEVICE = -8,    /* no CUDA device / wrong architecture */
+	NUCLEUS34_E_STATE = -9        /* call out of order (e.g. run before upload) */
+};
+
+enum
+{
+	NUCLEUS34_DIRECT = 0,    /* materialise four-cliques + triangle->clique CSR (cuNucleus34) */
+	NUCLEUS34_ONDEMAND = 1   /* edge->triangle incidence, re-enumerate at death (cuNucleus34_ondemand) */
+};
+
+/* ---- inputs and results ------------------------------------------------ */
+
+/* Oriented CSR on the HOST. O may be NULL (then built from D); when given it
+ * holds n entries, O[u] = first out-edge of u, like graph_t::O
+ * (nucleus/graph/graph.hpp:523-536). D[u] = out-degree, E = destinations. */
+typedef struct
+{
+	uint64_t n;
+	uint64_t m;
+	const uint32_t *O;
+	const uint32_t *D;
+	const uint32_t *E;
+} nucleus34_csr;
+
+typedef struct
+{
+	uint64_t mem_budget_bytes; /* 0 = 90% of the device's free memory */
+	int device;                /* CUDA ordinal */
+	uint32_t parts;            /* accepted for CLI parity (cuNucleus34.cu:161-169); one GPU */
+	const char *tune_table;    /* optional autotune table path, NULL = built-in defaults */
+} nucleus34_opts;
+
+typedef struct
+{
+	uint64_t triangle_count;
+	uint64_t four_clique_count;
+	uint64_t peeling_iterations;  /* peel rounds executed */
+	uint64_t unpeeled_count;      /* triangles left at -1 (0 on success) */
+	uint32_t k_max;
+	double k_avg;                 /* sum(k) / T, accumulated in 64-bit integers */
+	/* device-side phase times, seconds, CUDA events on the library stream */
+	double t_triangles;           /* triangle listing */
+	double t_incidence;           /* edge -> triangle incidence */
+	double t_support;             /* four-clique support count */
+	double t_cliques;             /* direct only: clique list + triangle->clique CSR */
+	double t_peel;                /* device-resident bucketed peel */
+	double t_total;               /* sum of the above (reference total_time_sec accounting) */
+	uint64_t incidence_entries;   /* 3 * triangle_count */
+	uint64_t gpu_launches;        /* kernels this run launched */
+	uint64_t peak_device_bytes;   /* high-water mark of the library's device allocations */
+	int variant;                  /* NUCLEUS34_DIRECT or NUCLEUS34_ONDEMAND */
+} nucleus34_result;
+
+typedef struct nucleus34_state *nucleus34_handle;
+
+/* ---- one-shot decomposition (drop-in for the two programs' device pipelines) */
+
+/* Replaces the device pipeline of the direct program, nucleus/cuNucleus34.cu:283-721
+ * (triangle listing, triangle graph, four-clique list, triangle->clique incidence,
+ * claim peel). Uploads the host CSR, runs on the device, keeps k (and the
+ * triangle and clique lists) behind *out until nucleus34_free. */
+int nucleus34_decompose(const nucleus34_csr *csr, const nucleus34_opts *opts,
+						nucleus34_result *res, nucleus34_handle *out);
+
+/* Replaces the device pipeline of nucleus/cuNucleus34_ondemand.cu:407-690
+ * (triangles, sorted incidence, support count, re-enumerating round peel). */
+int nucleus34_decompose_ondemand(const nucleus34_csr *csr, const nucleus34_opts *opts,
+								 nucleus34_result *res, nucleus34_handle *out);
+
+/* k_out: int32[triangle_count] in canonical order (may be NULL);
+ * tris_out: uint32[3*triangle_count] as (a,b,c) (may be NULL). */
+int nucleus34_copy_k(nucleus34_handle h, int32_t *k_out, uint32_t *tris_out);
+
+/* Direct variant only: count cliques starting at index first, each as four
+ * ascending triangle ids, in the library's canonical clique order (grouped by
+ * lowest member, then by the fourth vertex's id). */
+int nucleus34_copy_quds(nucleus34_handle h, uint64_t first, uint64_t count, uint32_t *quds_out);
+
+/* Writes the per-triangle file, one row "(a,b,c)\t<k>" per triangle in
+ * canonical order (layout of cuNucleus34_ondemand.cu:724-733). */
+int nucleus34_write_kfile(nucleus34_handle h, const char *path);
+
+void nucleus34_free(nucleus34_handle h);
+
+const char *nucleus34_strerror(int code);
+/* Detail of the calling thread's last failure ("" if none). */
+const char *nucleus34_last_error(void);
+
+/* ---- device-resident context (inputs stay in HBM across runs) ------------ */
+
+typedef struct nucleus34_ctx_s *nucleus34_ctx;
+
+int nucleus34_ctx_create(const nucleus34_opts *opts, nucleus34_ctx *out);
+/* H2D copy of the CSR into context-owned device memory (replaces the
+ * thrust::device_vector uploads, cuNucleus34.cu:290-293). */
+int nucleus34_ctx_upload(nucleus34_ctx ctx, const nucleus34_csr *csr);
+/* Runs one decomposition of the resident graph; results stay on the device. */
+int nucleus34_ctx_run(nucleus34_ctx ctx, int variant, nucleus34_result *res);
+int nucleus34_ctx_copy_k(nucleus34_ctx ctx, int32_t *k_out, uint32_t *tris_out);
+void nucleus34_ctx_destroy(nucleus34_ctx ctx);
+
+/* ---- host graph layer (reference reader/orientation semantics) ----------- */
+
+/* Library-owned oriented CSR; O has n+1 entries here. */
+typedef struct
+{
+	uint64_t n;
+	uint64_t m;
+	uint32_t *O;
+	uint32_t *D;
+	uint32_t *E;
+} nucleus34_graph;
+
+/* Dispatch by extension like the mains (cuNucleus34.cu:235-256):
+ * .mtx -> from_edges(mtx header) + make_oriented; .edges/.txt -> from_edges
+ * (first non-comment line consumed as a header, graph.hpp:307-318) +
+ * make_oriented; .grh -> deserialize + build_offset (already oriented). */
+int nucleus34_graph_load(const char *path, nucleus34_graph *g);
+/* Same semantics from an in-memory list (no header line): symmetrise, drop
+ * self-loops, sort + unique, n = max id + 1, orient (graph.hpp:356-411,176-218). */
+int nucleus34_graph_from_edges(const uint32_t *src, const uint32_t *dst, uint64_t count,
+							   nucleus34_graph *g);
+/* .grh writer (graph_t::serialize layout, graph.hpp:465-488). */
+int nucleus34_graph_save_grh(const nucleus34_graph *g, const char *path);
+void nucleus34_graph_release(nucleus34_graph *g);
+/* View of a loaded graph as the decomposition input. */
+nucleus34_csr nucleus34_graph_csr(const nucleus34_graph *g);
+
+/* ---- seeded synthetic inputs (no datasets on this system) ---------------- */
+
+typedef struct
+{
+	uint64_t count;
+	uint32_t *src;
+	uint32_t *dst;
+} nucleus34_edges;
+
+/* Each generator returns the cleaned undirected list: u < v, unique, no loops,
+ * sorted. Counter-based streams (splitmix64 of seed and index) make the output
+ * independent of the thread count. */
+int nucleus34_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+					   uint64_t seed, nucleus34_edges *out);
+int nucleus34_gen_rgg(uint64_t n, double expected_degree, uint64_t seed, nucleus34_edges *out);
+int nucleus34_gen_ws(uint64_t n, uint32_t k, double beta, uint64_t seed, nucleus34_edges *out);
+/* Bare .edges file with a sacrificial first line (a repeat of the first edge),
+ * so the reference reader's first-line drop loses nothing. */
+int nucleus34_edges_write(const nucleus34_edges *e, const char *path);
+void nucleus34_edges_release(nucleus34_edges *e);
+uint64_t nucleus34_splitmix64(uint64_t x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NUCLEUS34_H_ */
