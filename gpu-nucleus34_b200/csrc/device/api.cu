@@ -1,0 +1,580 @@
+// C-ABI of the decomposition: contexts (device, stream, budgeted memory,
+// resident graph), the pipeline driver and the result accessors.
+//
+// Reference counterparts: the two programs' device pipelines
+// (nucleus/cuNucleus34.cu:283-721, nucleus/cuNucleus34_ondemand.cu:407-690);
+// their CSR upload (cuNucleus34.cu:290-293) is nucleus34_ctx_upload, their
+// phase timers (hrc::now() around synchronised phases) become CUDA events on
+// the library stream.
+#include "pipeline.cuh"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include <omp.h>
+
+struct nucleus34_ctx_s
+{
+	n34::Ctx c;
+};
+
+struct nucleus34_state
+{
+	nucleus34_ctx ctx = nullptr;
+};
+
+namespace n34 {
+
+void clear_error();
+
+namespace {
+
+__global__ void k_validate(const uint32_t *__restrict__ O, const uint32_t *__restrict__ E, uint64_t n,
+						   uint32_t *__restrict__ bad)
+{
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	for (uint64_t u = warp; u < n; u += nwarps)
+	{
+		const uint32_t b = O[u], e = O[u + 1];
+		bool ok = b <= e;
+		for (uint32_t j = b + lane_id(); ok && j < e; j += 32)
+		{
+			const uint32_t v = E[j];
+			if (v >= n || v == u || (j > b && E[j - 1] >= v))
+				ok = false;
+		}
+		if (!ok)
+			atomicOr(bad, 1u);
+	}
+}
+
+__global__ void k_zero_k(int32_t *K, uint64_t T)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
+		K[t] = 0;
+}
+
+struct Events
+{
+	cudaEvent_t e[6] = {};
+	bool ok = true;
+	explicit Events()
+	{
+		for (auto &x : e)
+			ok = ok && cudaEventCreate(&x) == cudaSuccess;
+	}
+	~Events()
+	{
+		for (auto &x : e)
+			if (x)
+				cudaEventDestroy(x);
+	}
+	double sec(int a, int b)
+	{
+		float ms = 0.f;
+		if (cudaEventElapsedTime(&ms, e[a], e[b]) != cudaSuccess)
+			return 0.0;
+		return double(ms) * 1e-3;
+	}
+};
+
+int set_device(Ctx &c)
+{
+	N34_CUDA(cudaSetDevice(c.device));
+	return NUCLEUS34_OK;
+}
+
+} // namespace
+
+int Ctx::alloc(void **p, uint64_t bytes, const char *what)
+{
+	*p = nullptr;
+	if (bytes == 0)
+		bytes = 16;
+	bytes = (bytes + 255) & ~uint64_t(255);
+	if (in_use + bytes > budget)
+		return fail(NUCLEUS34_E_OOM_BUDGET, std::string("device memory budget exceeded allocating ") + what + " (" +
+												std::to_string(bytes >> 20) + " MiB; in use " +
+												std::to_string(in_use >> 20) + " of " + std::to_string(budget >> 20) +
+												" MiB)");
+	cudaError_t e = cudaMallocAsync(p, bytes, stream);
+	if (e != cudaSuccess)
+	{
+		cudaGetLastError();
+		*p = nullptr;
+		return fail(e == cudaErrorMemoryAllocation ? NUCLEUS34_E_OOM_BUDGET : NUCLEUS34_E_CUDA,
+					std::string("cudaMallocAsync ") + what + ": " + cudaGetErrorString(e));
+	}
+	in_use += bytes;
+	peak = std::max(peak, in_use);
+	sizes[*p] = bytes;
+	return NUCLEUS34_OK;
+}
+
+void Ctx::release(void *p)
+{
+	if (!p)
+		return;
+	auto it = sizes.find(p);
+	if (it != sizes.end())
+	{
+		in_use -= it->second;
+		sizes.erase(it);
+	}
+	cudaFreeAsync(p, stream);
+}
+
+void Ctx::release_results()
+{
+	release(dtris);
+	release(dK);
+	release(dquds);
+	dtris = nullptr;
+	dK = nullptr;
+	dquds = nullptr;
+	T = Q = 0;
+	have_result = false;
+}
+
+void Ctx::release_graph()
+{
+	release(dO);
+	release(dE);
+	release(dsrc);
+	dO = dE = dsrc = nullptr;
+	n = m = 0;
+}
+
+int upload(Ctx &c, const nucleus34_csr *csr)
+{
+	if (!csr || (csr->n && !csr->D) || (csr->m && !csr->E))
+		return fail(NUCLEUS34_E_INVALID, "null CSR array");
+	if (csr->m > 0xffffffffull || csr->n >= 0xffffffffull)
+		return fail(NUCLEUS34_E_RANGE32, "graph exceeds 32-bit vertex/edge ids");
+	N34_TRY(set_device(c));
+	c.release_results();
+	c.release_graph();
+	const uint64_t n = csr->n, m = csr->m;
+	std::vector<uint32_t> O(n + 1);
+	uint64_t s = 0;
+	for (uint64_t u = 0; u < n; ++u)
+	{
+		if (csr->O && csr->O[u] != s)
+			return fail(NUCLEUS34_E_INVALID, "O is not the exclusive scan of D");
+		O[u] = uint32_t(s);
+		s += csr->D[u];
+	}
+	if (s != m)
+		return fail(NUCLEUS34_E_INVALID, "sum of D does not equal m");
+	O[n] = uint32_t(m);
+	N34_TRY(dalloc(c, &c.dO, n + 1, "CSR offsets"));
+	N34_TRY(dalloc(c, &c.dE, m ? m : 1, "CSR destinations"));
+	N34_TRY(dalloc(c, &c.dsrc, m ? m : 1, "CSR sources"));
+	N34_CUDA(cudaMemcpyAsync(c.dO, O.data(), (n + 1) * 4, cudaMemcpyHostToDevice, c.stream));
+	if (m)
+		N34_CUDA(cudaMemcpyAsync(c.dE, csr->E, m * 4, cudaMemcpyHostToDevice, c.stream));
+	c.n = n;
+	c.m = m;
+	uint32_t *bad = nullptr;
+	N34_TRY(dalloc(c, &bad, 1, "validation flag"));
+	N34_CUDA(cudaMemsetAsync(bad, 0, 4, c.stream));
+	if (n)
+		N34_LAUNCH(c, k_validate, grid_for(c, n, 8), 256, 0, c.dO, c.dE, n, bad);
+	uint32_t hbad = 0;
+	N34_CUDA(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, c.stream));
+	N34_CUDA(cudaStreamSynchronize(c.stream));
+	c.release(bad);
+	if (hbad)
+	{
+		c.release_graph();
+		return fail(NUCLEUS34_E_INVALID,
+					"CSR adjacency must hold ids < n, no self-loops, strictly ascending per vertex");
+	}
+	N34_TRY(build_src(c));
+	N34_CUDA(cudaStreamSynchronize(c.stream));
+	return NUCLEUS34_OK;
+}
+
+int run(Ctx &c, int variant, nucleus34_result *out)
+{
+	if (variant != NUCLEUS34_DIRECT && variant != NUCLEUS34_ONDEMAND)
+		return fail(NUCLEUS34_E_INVALID, "unknown variant");
+	if (!c.dO)
+		return fail(NUCLEUS34_E_STATE, "no graph uploaded");
+	N34_TRY(set_device(c));
+	c.release_results();
+	const uint64_t launches0 = c.launches;
+	c.peak = c.in_use;
+	Events ev;
+	if (!ev.ok)
+		return fail(NUCLEUS34_E_CUDA, "event creation");
+	nucleus34_result r{};
+	r.variant = variant;
+	Incidence inc;
+	CliqueCsr csr;
+	int32_t *S = nullptr;
+	int rc = NUCLEUS34_OK;
+	PeelCtl pc{};
+	bool peeled = false;
+	do
+	{
+		N34_CUDA(cudaEventRecord(ev.e[0], c.stream));
+		if ((rc = list_triangles(c)))
+			break;
+		N34_CUDA(cudaEventRecord(ev.e[1], c.stream));
+		r.triangle_count = c.T;
+		r.incidence_entries = 3 * c.T;
+		if (c.T)
+		{
+			if ((rc = build_incidence(c, inc)))
+				break;
+		}
+		N34_CUDA(cudaEventRecord(ev.e[2], c.stream));
+		uint64_t total = 0;
+		if (c.T)
+		{
+			if ((rc = dalloc(c, &S, c.T, "support")))
+				break;
+			if ((rc = count_support(c, inc, S, &total)))
+				break;
+			if (total % 4)
+			{
+				rc = fail(NUCLEUS34_E_CUDA, "internal: clique incidences not a multiple of 4");
+				break;
+			}
+		}
+		r.four_clique_count = total / 4;
+		N34_CUDA(cudaEventRecord(ev.e[3], c.stream));
+		if (variant == NUCLEUS34_DIRECT && total)
+		{
+			if ((rc = list_cliques(c, inc, S, csr)))
+				break;
+			if (c.Q != total / 4)
+			{
+				rc = fail(NUCLEUS34_E_CUDA, "internal: clique list size differs from support total");
+				break;
+			}
+		}
+		if (variant == NUCLEUS34_DIRECT)
+			free_incidence(c, inc);
+		N34_CUDA(cudaEventRecord(ev.e[4], c.stream));
+		if (c.T)
+		{
+			if ((rc = dalloc(c, &c.dK, c.T, "k values")))
+				break;
+			if (total)
+			{
+				if ((rc = peel(c, variant, inc, csr, S, c.dK, &pc)))
+					break;
+				peeled = true;
+			}
+			else
+			{
+				N34_LAUNCH(c, k_zero_k, grid_for(c, c.T, 256), 256, 0, c.dK, c.T);
+			}
+		}
+		N34_CUDA(cudaEventRecord(ev.e[5], c.stream));
+		N34_CUDA(cudaStreamSynchronize(c.stream));
+	} while (false);
+	free_incidence(c, inc);
+	free_clique_csr(c, csr);
+	c.release(S);
+	if (rc)
+	{
+		c.release_results();
+		cudaStreamSynchronize(c.stream);
+		return rc;
+	}
+	r.t_triangles = ev.sec(0, 1);
+	r.t_incidence = ev.sec(1, 2);
+	r.t_support = ev.sec(2, 3);
+	r.t_cliques = ev.sec(3, 4);
+	r.t_peel = ev.sec(4, 5);
+	r.t_total = r.t_triangles + r.t_incidence + r.t_support + r.t_cliques + r.t_peel;
+	if (peeled)
+	{
+		r.peeling_iterations = pc.rounds;
+		r.unpeeled_count = pc.unpeeled;
+		r.k_max = pc.kmax;
+		r.k_avg = c.T ? double(pc.ksum) / double(c.T) : 0.0;
+	}
+	r.gpu_launches = c.launches - launches0;
+	r.peak_device_bytes = c.peak;
+	c.variant = variant;
+	c.have_result = true;
+	c.res = r;
+	if (out)
+		*out = r;
+	return NUCLEUS34_OK;
+}
+
+int copy_k(Ctx &c, int32_t *k_out, uint32_t *tris_out)
+{
+	if (!c.have_result)
+		return fail(NUCLEUS34_E_STATE, "no result");
+	N34_TRY(set_device(c));
+	if (k_out && c.T)
+		N34_CUDA(cudaMemcpyAsync(k_out, c.dK, c.T * 4, cudaMemcpyDeviceToHost, c.stream));
+	if (tris_out && c.T)
+		N34_CUDA(cudaMemcpyAsync(tris_out, c.dtris, c.T * 12, cudaMemcpyDeviceToHost, c.stream));
+	N34_CUDA(cudaStreamSynchronize(c.stream));
+	return NUCLEUS34_OK;
+}
+
+int write_kfile(Ctx &c, const char *path)
+{
+	std::vector<int32_t> k(c.T);
+	std::vector<uint32_t> t(3 * c.T);
+	N34_TRY(copy_k(c, k.data(), t.data()));
+	FILE *f = std::fopen(path, "wb");
+	if (!f)
+		return fail(NUCLEUS34_E_IO, std::string("Failed to open output file: ") + path);
+	const uint64_t T = c.T, chunk = 1u << 18;
+	const uint64_t nchunks = (T + chunk - 1) / chunk;
+	bool ok = true;
+	// format chunks in parallel, write them in order
+	for (uint64_t c0 = 0; c0 < nchunks && ok; c0 += 64)
+	{
+		const uint64_t c1 = std::min(nchunks, c0 + 64);
+		std::vector<std::string> bufs(c1 - c0);
+#pragma omp parallel for schedule(dynamic, 1)
+		for (int64_t ci = int64_t(c0); ci < int64_t(c1); ++ci)
+		{
+			std::string &b = bufs[size_t(ci - int64_t(c0))];
+			const uint64_t s = uint64_t(ci) * chunk, e = std::min(T, s + chunk);
+			b.reserve((e - s) * 40);
+			char line[64];
+			for (uint64_t i = s; i < e; ++i)
+			{
+				const int len = std::snprintf(line, sizeof(line), "(%u,%u,%u)\t%d\n", t[3 * i], t[3 * i + 1],
+											  t[3 * i + 2], k[i]);
+				b.append(line, size_t(len));
+			}
+		}
+		for (auto &b : bufs)
+			ok = ok && std::fwrite(b.data(), 1, b.size(), f) == b.size();
+	}
+	ok = (std::fclose(f) == 0) && ok;
+	return ok ? NUCLEUS34_OK : fail(NUCLEUS34_E_IO, "short write");
+}
+
+int create_ctx(const nucleus34_opts *opts, nucleus34_ctx *out)
+{
+	*out = nullptr;
+	int dev = opts ? opts->device : 0;
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+	{
+		cudaGetLastError();
+		return fail(NUCLEUS34_E_NODEVICE, "no CUDA device visible");
+	}
+	if (dev < 0 || dev >= ndev)
+		return fail(NUCLEUS34_E_INVALID, "device ordinal out of range");
+	cudaDeviceProp prop{};
+	N34_CUDA(cudaGetDeviceProperties(&prop, dev));
+	if (prop.major < 10)
+		return fail(NUCLEUS34_E_NODEVICE, std::string("this build targets sm_100a; device is ") + prop.name);
+	N34_CUDA(cudaSetDevice(dev));
+	auto *x = new (std::nothrow) nucleus34_ctx_s();
+	if (!x)
+		return fail(NUCLEUS34_E_INVALID, "host allocation failed");
+	Ctx &c = x->c;
+	c.device = dev;
+	c.sm_count = prop.multiProcessorCount;
+	if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
+	{
+		delete x;
+		return fail(NUCLEUS34_E_CUDA, "stream creation");
+	}
+	size_t fb = 0, tb = 0;
+	cudaMemGetInfo(&fb, &tb);
+	c.budget = (opts && opts->mem_budget_bytes) ? opts->mem_budget_bytes : uint64_t(double(fb) * 0.9);
+	if (opts && opts->tune_table)
+		c.tune_table = opts->tune_table;
+	*out = x;
+	return NUCLEUS34_OK;
+}
+
+void destroy_ctx(nucleus34_ctx x)
+{
+	if (!x)
+		return;
+	Ctx &c = x->c;
+	cudaSetDevice(c.device);
+	c.release_results();
+	c.release_graph();
+	for (auto &kv : c.sizes)
+		cudaFreeAsync(kv.first, c.stream);
+	c.sizes.clear();
+	if (c.stream)
+	{
+		cudaStreamSynchronize(c.stream);
+		cudaStreamDestroy(c.stream);
+	}
+	delete x;
+}
+
+template <class F>
+int guarded(F &&f)
+{
+	clear_error();
+	try
+	{
+		return f();
+	}
+	catch (const std::bad_alloc &)
+	{
+		return fail(NUCLEUS34_E_INVALID, "host allocation failed");
+	}
+	catch (const std::exception &e)
+	{
+		return fail(NUCLEUS34_E_INVALID, e.what());
+	}
+	catch (...)
+	{
+		return fail(NUCLEUS34_E_INVALID, "unknown error");
+	}
+}
+
+int decompose_impl(const nucleus34_csr *csr, const nucleus34_opts *opts, nucleus34_result *res,
+				   nucleus34_handle *out, int variant)
+{
+	if (!out)
+		return fail(NUCLEUS34_E_INVALID, "null handle output");
+	*out = nullptr;
+	nucleus34_ctx ctx = nullptr;
+	N34_TRY(create_ctx(opts, &ctx));
+	int rc;
+	{
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		rc = upload(ctx->c, csr);
+		if (!rc)
+			rc = run(ctx->c, variant, res);
+	}
+	if (rc)
+	{
+		destroy_ctx(ctx);
+		return rc;
+	}
+	auto *h = new (std::nothrow) nucleus34_state();
+	if (!h)
+	{
+		destroy_ctx(ctx);
+		return fail(NUCLEUS34_E_INVALID, "host allocation failed");
+	}
+	h->ctx = ctx;
+	*out = h;
+	return NUCLEUS34_OK;
+}
+
+} // namespace n34
+
+using namespace n34;
+
+extern "C" {
+
+int nucleus34_ctx_create(const nucleus34_opts *opts, nucleus34_ctx *out)
+{
+	if (!out)
+		return fail(NUCLEUS34_E_INVALID, "null output");
+	return guarded([&] { return create_ctx(opts, out); });
+}
+
+int nucleus34_ctx_upload(nucleus34_ctx ctx, const nucleus34_csr *csr)
+{
+	if (!ctx)
+		return fail(NUCLEUS34_E_INVALID, "null context");
+	return guarded([&] {
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		return upload(ctx->c, csr);
+	});
+}
+
+int nucleus34_ctx_run(nucleus34_ctx ctx, int variant, nucleus34_result *res)
+{
+	if (!ctx)
+		return fail(NUCLEUS34_E_INVALID, "null context");
+	return guarded([&] {
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		return run(ctx->c, variant, res);
+	});
+}
+
+int nucleus34_ctx_copy_k(nucleus34_ctx ctx, int32_t *k_out, uint32_t *tris_out)
+{
+	if (!ctx)
+		return fail(NUCLEUS34_E_INVALID, "null context");
+	return guarded([&] {
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		return copy_k(ctx->c, k_out, tris_out);
+	});
+}
+
+void nucleus34_ctx_destroy(nucleus34_ctx ctx) { destroy_ctx(ctx); }
+
+int nucleus34_decompose(const nucleus34_csr *csr, const nucleus34_opts *opts, nucleus34_result *res,
+						nucleus34_handle *out)
+{
+	return guarded([&] { return decompose_impl(csr, opts, res, out, NUCLEUS34_DIRECT); });
+}
+
+int nucleus34_decompose_ondemand(const nucleus34_csr *csr, const nucleus34_opts *opts, nucleus34_result *res,
+								 nucleus34_handle *out)
+{
+	return guarded([&] { return decompose_impl(csr, opts, res, out, NUCLEUS34_ONDEMAND); });
+}
+
+int nucleus34_copy_k(nucleus34_handle h, int32_t *k_out, uint32_t *tris_out)
+{
+	if (!h || !h->ctx)
+		return fail(NUCLEUS34_E_INVALID, "null handle");
+	return nucleus34_ctx_copy_k(h->ctx, k_out, tris_out);
+}
+
+int nucleus34_copy_quds(nucleus34_handle h, uint64_t first, uint64_t count, uint32_t *quds_out)
+{
+	if (!h || !h->ctx || (count && !quds_out))
+		return fail(NUCLEUS34_E_INVALID, "null argument");
+	return guarded([&] {
+		Ctx &c = h->ctx->c;
+		std::lock_guard<std::mutex> lk(c.mu);
+		if (!c.have_result || c.variant != NUCLEUS34_DIRECT)
+			return fail(NUCLEUS34_E_STATE, "four-clique list exists only after a direct decomposition");
+		if (first > c.Q || count > c.Q - first)
+			return fail(NUCLEUS34_E_INVALID, "clique range out of bounds");
+		if (!count)
+			return int(NUCLEUS34_OK);
+		N34_TRY(set_device(c));
+		N34_CUDA(cudaMemcpyAsync(quds_out, c.dquds + 4 * first, count * 16, cudaMemcpyDeviceToHost, c.stream));
+		N34_CUDA(cudaStreamSynchronize(c.stream));
+		return int(NUCLEUS34_OK);
+	});
+}
+
+int nucleus34_write_kfile(nucleus34_handle h, const char *path)
+{
+	if (!h || !h->ctx || !path)
+		return fail(NUCLEUS34_E_INVALID, "null argument");
+	return guarded([&] {
+		std::lock_guard<std::mutex> lk(h->ctx->c.mu);
+		return write_kfile(h->ctx->c, path);
+	});
+}
+
+void nucleus34_free(nucleus34_handle h)
+{
+	if (!h)
+		return;
+	destroy_ctx(h->ctx);
+	delete h;
+}
+
+} // extern "C"

@@ -1,0 +1,335 @@
+// Edge -> triangle incidence: for every oriented edge e, the triangles that
+// contain e, each as (third vertex x, triangle id), sorted by x.
+//
+// Reference: build_incidence_entries + thrust::sort_by_key on the 64-bit key
+// (edge<<32 | third) + split_keys + lower_bound (nucleus/cuNucleus34_ondemand.cu:
+// 92-128, 513-549): one global radix sort of 3T 64-bit keys.
+//
+// Here: per-edge counts (atomics) -> exclusive scan -> scatter of 64-bit
+// (x<<32 | t) entries into their edge's segment -> a segmented sort of each
+// segment by x (segments are short: a warp bitonic network for <= 32 entries,
+// a shared-memory block bitonic sort up to SEG_SMEM, a global-memory bitonic
+// sort on a padded copy beyond that) -> split into the third[] and tri[]
+// arrays the 3-way intersection reads. Triangle t = (a,b,c) with u = src[b],
+// v = E[b], w = E[c] is listed under b with x = w, under a with x = v and under
+// c with x = u, exactly the reference's three entries.
+#include "pipeline.cuh"
+
+#include <algorithm>
+
+namespace n34 {
+
+namespace {
+
+constexpr int SEG_SMEM = 8192;        // keys per block sort (64 KB smem)
+constexpr int SEG_BLOCK = 512;
+
+__global__ void k_inc_count(const uint32_t *__restrict__ tris, uint64_t T, uint32_t *__restrict__ cnt)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
+	{
+		atomicAdd(cnt + tris[3 * t + 0], 1u);
+		atomicAdd(cnt + tris[3 * t + 1], 1u);
+		atomicAdd(cnt + tris[3 * t + 2], 1u);
+	}
+}
+
+__global__ void k_inc_scatter(const uint32_t *__restrict__ tris, uint64_t T, const uint32_t *__restrict__ src,
+							  const uint32_t *__restrict__ E, const uint64_t *__restrict__ incO,
+							  uint32_t *__restrict__ cursor, unsigned long long *__restrict__ keys,
+							  uint32_t *__restrict__ err)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
+	{
+		const uint32_t a = tris[3 * t + 0], b = tris[3 * t + 1], c = tris[3 * t + 2];
+		const uint32_t u = src[b], v = E[b], w = E[c];
+		const uint32_t e3[3] = {b, a, c};
+		const uint32_t x3[3] = {w, v, u};
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+		{
+			const uint32_t e = e3[r];
+			const uint32_t s = atomicAdd(cursor + e, 1u);
+			// capacity guard: the counts pass sized every segment exactly
+			if (incO[e] + s < incO[e + 1])
+				keys[incO[e] + s] = (uint64_t(x3[r]) << 32) | t;
+			else
+				atomicOr(err, 1u);
+		}
+	}
+}
+
+// Classifies edges by segment length into three work lists.
+__global__ void k_seg_classify(const uint64_t *__restrict__ incO, uint64_t m, uint32_t *__restrict__ lists,
+							   uint32_t *__restrict__ counts, uint64_t list_cap, unsigned long long *max_len)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t e0 = uint64_t(blockIdx.x) * blockDim.x; e0 < m; e0 += stride)
+	{
+		const uint64_t e = e0 + threadIdx.x;
+		uint64_t len = 0;
+		if (e < m)
+			len = incO[e + 1] - incO[e];
+		const int cls = len < 2 ? -1 : (len <= 32 ? 0 : (len <= SEG_SMEM ? 1 : 2));
+#pragma unroll
+		for (int k = 0; k < 3; ++k)
+		{
+			const uint32_t slot = warp_append(cls == k, counts + k);
+			if (cls == k)
+				lists[uint64_t(k) * list_cap + slot] = uint32_t(e);
+		}
+		if (cls == 2)
+			atomicMax(max_len, (unsigned long long)len);
+	}
+}
+
+// Warp per segment (<= 32 entries): register bitonic network.
+__global__ void k_seg_sort_warp(const uint32_t *__restrict__ list, const uint32_t *__restrict__ count,
+								const uint64_t *__restrict__ incO, unsigned long long *__restrict__ keys)
+{
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	const uint32_t n = *count;
+	const uint32_t lane = lane_id();
+	for (uint64_t i = warp; i < n; i += nwarps)
+	{
+		const uint32_t e = list[i];
+		const uint64_t b = incO[e], len = incO[e + 1] - b;
+		unsigned long long k = lane < len ? keys[b + lane] : ~0ull;
+#pragma unroll
+		for (int size = 2; size <= 32; size <<= 1)
+		{
+#pragma unroll
+			for (int stride = size >> 1; stride > 0; stride >>= 1)
+			{
+				const unsigned long long o = __shfl_xor_sync(FULL, k, stride);
+				const bool up = (lane & size) == 0;
+				const bool lower = (lane & stride) == 0;
+				const unsigned long long mn = k < o ? k : o, mx = k < o ? o : k;
+				k = (lower == up) ? mn : mx;
+			}
+		}
+		if (lane < len)
+			keys[b + lane] = k;
+	}
+}
+
+// Block bitonic sort of n (padded to pow2 P) keys in `s` (shared or global).
+__device__ __forceinline__ void block_bitonic(unsigned long long *s, uint32_t P)
+{
+	for (uint32_t size = 2; size <= P; size <<= 1)
+		for (uint32_t stride = size >> 1; stride > 0; stride >>= 1)
+		{
+			for (uint32_t i = threadIdx.x; i < P / 2; i += blockDim.x)
+			{
+				const uint32_t lo = 2 * i - (i & (stride - 1));
+				const uint32_t hi = lo + stride;
+				const bool up = (lo & size) == 0;
+				unsigned long long x = s[lo], y = s[hi];
+				if ((x > y) == up)
+				{
+					s[lo] = y;
+					s[hi] = x;
+				}
+			}
+			__syncthreads();
+		}
+}
+
+__global__ void __launch_bounds__(SEG_BLOCK) k_seg_sort_block(const uint32_t *__restrict__ list,
+															  const uint32_t *__restrict__ count,
+															  const uint64_t *__restrict__ incO,
+															  unsigned long long *__restrict__ keys)
+{
+	extern __shared__ unsigned long long sm[];
+	const uint32_t n = *count;
+	for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
+	{
+		const uint32_t e = list[i];
+		const uint64_t b = incO[e];
+		const uint32_t len = uint32_t(incO[e + 1] - b);
+		uint32_t P = 64;
+		while (P < len)
+			P <<= 1;
+		for (uint32_t j = threadIdx.x; j < P; j += blockDim.x)
+			sm[j] = j < len ? keys[b + j] : ~0ull;
+		__syncthreads();
+		block_bitonic(sm, P);
+		for (uint32_t j = threadIdx.x; j < len; j += blockDim.x)
+			keys[b + j] = sm[j];
+		__syncthreads();
+	}
+}
+
+// Long segments: padded copy in global scratch (one region per block).
+__global__ void __launch_bounds__(SEG_BLOCK) k_seg_sort_global(const uint32_t *__restrict__ list,
+															   const uint32_t *__restrict__ count,
+															   const uint64_t *__restrict__ incO,
+															   unsigned long long *__restrict__ keys,
+															   unsigned long long *__restrict__ scratch,
+															   uint64_t region)
+{
+	const uint32_t n = *count;
+	unsigned long long *s = scratch + uint64_t(blockIdx.x) * region;
+	for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
+	{
+		const uint32_t e = list[i];
+		const uint64_t b = incO[e];
+		const uint64_t len = incO[e + 1] - b;
+		uint64_t P = 64;
+		while (P < len)
+			P <<= 1;
+		if (P > region)
+			continue; // cannot happen: region is sized from the longest segment
+		for (uint64_t j = threadIdx.x; j < P; j += blockDim.x)
+			s[j] = j < len ? keys[b + j] : ~0ull;
+		__syncthreads();
+		block_bitonic(s, uint32_t(P));
+		for (uint64_t j = threadIdx.x; j < len; j += blockDim.x)
+			keys[b + j] = s[j];
+		__syncthreads();
+	}
+}
+
+__global__ void k_inc_split(const unsigned long long *__restrict__ keys, uint64_t n, uint32_t *__restrict__ third,
+							uint32_t *__restrict__ tri)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+	{
+		const unsigned long long k = keys[i];
+		third[i] = uint32_t(k >> 32);
+		tri[i] = uint32_t(k);
+	}
+}
+
+} // namespace
+
+int build_incidence(Ctx &c, Incidence &inc)
+{
+	const uint64_t T = c.T, m = c.m, n3 = 3 * T;
+	uint32_t *cnt = nullptr, *lists = nullptr, *counts = nullptr, *errf = nullptr;
+	unsigned long long *keys = nullptr, *scratch = nullptr, *maxlen = nullptr;
+	int rc = NUCLEUS34_OK;
+	auto cleanup = [&] {
+		c.release(cnt);
+		c.release(lists);
+		c.release(counts);
+		c.release(keys);
+		c.release(scratch);
+		c.release(maxlen);
+		c.release(errf);
+	};
+	do
+	{
+		if ((rc = dalloc(c, &inc.off, m + 1, "incidence offsets")))
+			break;
+		if ((rc = dalloc(c, &cnt, m, "incidence counts")))
+			break;
+		if (cudaMemsetAsync(cnt, 0, m * 4, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "memset");
+			break;
+		}
+		k_inc_count<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, cnt);
+		c.launches++;
+		if ((rc = scan_u32(c, cnt, inc.off, m)))
+			break;
+		if ((rc = dalloc(c, &keys, n3, "incidence keys")))
+			break;
+		if (cudaMemsetAsync(cnt, 0, m * 4, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "memset");
+			break;
+		}
+		if ((rc = dalloc(c, &errf, 1, "incidence check")))
+			break;
+		if (cudaMemsetAsync(errf, 0, 4, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "memset");
+			break;
+		}
+		k_inc_scatter<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, c.dsrc, c.dE, inc.off, cnt, keys, errf);
+		c.launches++;
+		c.release(cnt);
+		cnt = nullptr;
+		// segmented sort
+		if ((rc = dalloc(c, &lists, 3 * m, "segment lists")))
+			break;
+		if ((rc = dalloc(c, &counts, 4, "segment counts")))
+			break;
+		if ((rc = dalloc(c, &maxlen, 1, "segment max")))
+			break;
+		if (cudaMemsetAsync(counts, 0, 16, c.stream) != cudaSuccess ||
+			cudaMemsetAsync(maxlen, 0, 8, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "memset");
+			break;
+		}
+		k_seg_classify<<<grid_for(c, m, 256), 256, 0, c.stream>>>(inc.off, m, lists, counts, m, maxlen);
+		c.launches++;
+		uint32_t hcounts[4] = {0, 0, 0, 0};
+		unsigned long long hmax = 0;
+		uint32_t herr = 0;
+		if (cudaMemcpyAsync(&herr, errf, 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaMemcpyAsync(hcounts, counts, 16, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaMemcpyAsync(&hmax, maxlen, 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "segment classify");
+			break;
+		}
+		if (herr)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "internal: incidence segment overflow");
+			break;
+		}
+		if (hcounts[0])
+		{
+			k_seg_sort_warp<<<grid_for(c, hcounts[0], 8, 32), 256, 0, c.stream>>>(lists, counts + 0, inc.off, keys);
+			c.launches++;
+		}
+		if (hcounts[1])
+		{
+			const size_t smem = SEG_SMEM * sizeof(unsigned long long);
+			cudaFuncSetAttribute(k_seg_sort_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+			k_seg_sort_block<<<grid_for(c, hcounts[1], 1, 2), SEG_BLOCK, smem, c.stream>>>(lists + m, counts + 1,
+																							inc.off, keys);
+			c.launches++;
+		}
+		if (hcounts[2])
+		{
+			uint64_t P = 64;
+			while (P < hmax)
+				P <<= 1;
+			const uint32_t blocks = std::min<uint32_t>(hcounts[2], uint32_t(c.sm_count));
+			if ((rc = dalloc(c, &scratch, P * blocks, "segment sort scratch")))
+				break;
+			k_seg_sort_global<<<blocks, SEG_BLOCK, 0, c.stream>>>(lists + 2 * m, counts + 2, inc.off, keys,
+																  scratch, P);
+			c.launches++;
+		}
+		if ((rc = dalloc(c, &inc.third, n3, "incidence third")))
+			break;
+		if ((rc = dalloc(c, &inc.tri, n3, "incidence tri")))
+			break;
+		k_inc_split<<<grid_for(c, n3, 256), 256, 0, c.stream>>>(keys, n3, inc.third, inc.tri);
+		c.launches++;
+		if (cudaGetLastError() != cudaSuccess)
+			rc = fail(NUCLEUS34_E_CUDA, "incidence kernels");
+	} while (false);
+	cleanup();
+	return rc;
+}
+
+void free_incidence(Ctx &c, Incidence &inc)
+{
+	c.release(inc.off);
+	c.release(inc.third);
+	c.release(inc.tri);
+	inc = Incidence{};
+}
+
+} // namespace n34

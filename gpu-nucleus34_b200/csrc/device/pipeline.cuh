@@ -1,0 +1,36 @@
+// Stages of the device pipeline and the data they hand to each other.
+#pragma once
+
+#include "common.cuh"
+
+namespace n34 {
+
+// Edge -> triangle incidence, per edge sorted by third vertex.
+struct Incidence
+{
+	uint64_t *off = nullptr;   // m+1
+	uint32_t *third = nullptr; // 3T
+	uint32_t *tri = nullptr;   // 3T
+};
+
+// Triangle -> four-clique incidence of the direct variant.
+struct CliqueCsr
+{
+	uint64_t *off = nullptr; // T+1
+	uint32_t *ids = nullptr; // 4Q clique ids
+};
+
+int build_src(Ctx &c);
+int list_triangles(Ctx &c);
+int build_incidence(Ctx &c, Incidence &inc);
+void free_incidence(Ctx &c, Incidence &inc);
+// support[t] = number of four-cliques on t; returns sum(support) in *total.
+int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total);
+// Direct variant: canonical clique list (c.dquds, c.Q) and triangle->clique CSR.
+int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, CliqueCsr &csr);
+void free_clique_csr(Ctx &c, CliqueCsr &csr);
+// Device-resident peel; K receives the final k of every triangle.
+int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_t *support, int32_t *K,
+		 PeelCtl *hctl);
+
+} // namespace n34

@@ -1,0 +1,303 @@
+// Four-clique support per triangle, and the direct variant's clique list and
+// triangle -> clique CSR.
+//
+// Reference: count_support (nucleus/cuNucleus34_ondemand.cu:176-194) counts
+// cliques per triangle through the 3-way zipper; the direct program lists the
+// cliques over the triangle graph (cu_cliques_quds, nucleus/utils.cuh:550-619)
+// in atomic order and builds the triangle -> clique incidence by
+// sort_by_key + lower_bound (cuNucleus34.cu:627-669).
+//
+// Here: one warp per triangle runs the 3-way intersection (intersect.cuh).
+// Every clique is listed once, by its lowest triangle id, in ascending order of
+// its fourth vertex: a count pass, a scan and a write pass give a
+// deterministic clique order with no sort. The triangle -> clique CSR uses the
+// supports as counts (support[t] = cliques on t), a scan, and an atomic
+// scatter of clique ids (the order inside a triangle's list does not affect
+// the peel result).
+#include "intersect.cuh"
+#include "pipeline.cuh"
+
+namespace n34 {
+
+namespace {
+
+constexpr int SUP_THREADS = 256;
+
+struct TriEdges
+{
+	uint64_t b0, e0, b1, e1, b2, e2;
+};
+
+__device__ __forceinline__ TriEdges tri_lists(const uint32_t *__restrict__ tris, const uint64_t *__restrict__ incO,
+											  uint64_t t)
+{
+	const uint32_t a = __ldg(tris + 3 * t + 0), b = __ldg(tris + 3 * t + 1), c = __ldg(tris + 3 * t + 2);
+	TriEdges L;
+	L.b0 = incO[a];
+	L.e0 = incO[a + 1];
+	L.b1 = incO[b];
+	L.e1 = incO[b + 1];
+	L.b2 = incO[c];
+	L.e2 = incO[c + 1];
+	return L;
+}
+
+__global__ void __launch_bounds__(SUP_THREADS) k_support(const uint32_t *__restrict__ tris, uint64_t T,
+														 const uint64_t *__restrict__ incO,
+														 const uint32_t *__restrict__ third,
+														 int32_t *__restrict__ support,
+														 unsigned long long *__restrict__ total)
+{
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	unsigned long long acc = 0;
+	for (uint64_t t = warp; t < T; t += nwarps)
+	{
+		const TriEdges L = tri_lists(tris, incO, t);
+		uint32_t cnt = 0;
+		warp_intersect3(third, L.b0, L.e0, L.b1, L.e1, L.b2, L.e2,
+						[&](bool found, uint32_t, uint64_t, uint64_t, uint64_t) {
+							cnt += __popc(__ballot_sync(FULL, found));
+						});
+		if (lane_id() == 0)
+		{
+			support[t] = int32_t(cnt);
+			acc += cnt;
+		}
+	}
+	if (lane_id() == 0 && acc)
+		atomicAdd(total, acc);
+}
+
+// own[t] = cliques whose lowest triangle is t
+__global__ void __launch_bounds__(SUP_THREADS) k_clique_own(const uint32_t *__restrict__ tris, uint64_t T,
+															const uint64_t *__restrict__ incO,
+															const uint32_t *__restrict__ third,
+															const uint32_t *__restrict__ itri,
+															uint32_t *__restrict__ own)
+{
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	for (uint64_t t = warp; t < T; t += nwarps)
+	{
+		const TriEdges L = tri_lists(tris, incO, t);
+		uint32_t cnt = 0;
+		warp_intersect3(third, L.b0, L.e0, L.b1, L.e1, L.b2, L.e2,
+						[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+							bool mine = false;
+							if (found)
+							{
+								const uint32_t q0 = __ldg(itri + pd), q1 = __ldg(itri + p1), q2 = __ldg(itri + p2);
+								mine = uint32_t(t) < q0 && uint32_t(t) < q1 && uint32_t(t) < q2;
+							}
+							cnt += __popc(__ballot_sync(FULL, mine));
+						});
+		if (lane_id() == 0)
+			own[t] = cnt;
+	}
+}
+
+__device__ __forceinline__ void sort3(uint32_t &a, uint32_t &b, uint32_t &c)
+{
+	uint32_t t;
+	if (a > b)
+	{
+		t = a;
+		a = b;
+		b = t;
+	}
+	if (b > c)
+	{
+		t = b;
+		b = c;
+		c = t;
+	}
+	if (a > b)
+	{
+		t = a;
+		a = b;
+		b = t;
+	}
+}
+
+__global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__restrict__ tris, uint64_t T,
+															  const uint64_t *__restrict__ incO,
+															  const uint32_t *__restrict__ third,
+															  const uint32_t *__restrict__ itri,
+															  const uint64_t *__restrict__ qoff,
+															  uint4 *__restrict__ quds)
+{
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	for (uint64_t t = warp; t < T; t += nwarps)
+	{
+		uint64_t out = qoff[t];
+		const uint64_t out_end = qoff[t + 1];
+		if (out == out_end)
+			continue;
+		const TriEdges L = tri_lists(tris, incO, t);
+		warp_intersect3(third, L.b0, L.e0, L.b1, L.e1, L.b2, L.e2,
+						[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+							bool mine = false;
+							uint32_t q0 = 0, q1 = 0, q2 = 0;
+							if (found)
+							{
+								q0 = __ldg(itri + pd);
+								q1 = __ldg(itri + p1);
+								q2 = __ldg(itri + p2);
+								mine = uint32_t(t) < q0 && uint32_t(t) < q1 && uint32_t(t) < q2;
+							}
+							const uint32_t word = __ballot_sync(FULL, mine);
+							const uint64_t at = out + __popc(word & lanemask_lt());
+							if (mine && at < out_end) // capacity guard (the count pass sized it)
+							{
+								sort3(q0, q1, q2);
+								quds[at] = make_uint4(uint32_t(t), q0, q1, q2);
+							}
+							out += __popc(word);
+						});
+	}
+}
+
+__global__ void k_clique_fill(const uint4 *__restrict__ quds, uint64_t Q, const uint64_t *__restrict__ coff,
+							  uint32_t *__restrict__ cursor, uint32_t *__restrict__ ids, uint32_t *__restrict__ err)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t q = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; q < Q; q += stride)
+	{
+		const uint4 x = quds[q];
+		const uint32_t m4[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+		for (int r = 0; r < 4; ++r)
+		{
+			const uint64_t at = coff[m4[r]] + atomicAdd(cursor + m4[r], 1u);
+			// capacity guard: counts are the supports, which list every clique of t once
+			if (at < coff[m4[r] + 1])
+				ids[at] = uint32_t(q);
+			else
+				atomicOr(err, 1u);
+		}
+	}
+}
+
+} // namespace
+
+int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total)
+{
+	unsigned long long *dtot = nullptr;
+	N34_TRY(dalloc(c, &dtot, 1, "support total"));
+	int rc = NUCLEUS34_OK;
+	do
+	{
+		if (cudaMemsetAsync(dtot, 0, 8, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "memset");
+			break;
+		}
+		k_support<<<grid_for(c, c.T, SUP_THREADS / 32, 32), SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.off,
+																						 inc.third, support, dtot);
+		c.launches++;
+		unsigned long long h = 0;
+		if (cudaGetLastError() != cudaSuccess ||
+			cudaMemcpyAsync(&h, dtot, 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "support count");
+			break;
+		}
+		*total = h;
+	} while (false);
+	c.release(dtot);
+	return rc;
+}
+
+int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, CliqueCsr &csr)
+{
+	const uint64_t T = c.T;
+	uint32_t *own = nullptr, *cursor = nullptr, *errf = nullptr;
+	uint64_t *qoff = nullptr;
+	int rc = NUCLEUS34_OK;
+	auto cleanup = [&] {
+		c.release(own);
+		c.release(cursor);
+		c.release(qoff);
+		c.release(errf);
+	};
+	do
+	{
+		if ((rc = dalloc(c, &own, T, "clique owner counts")))
+			break;
+		if ((rc = dalloc(c, &qoff, T + 1, "clique offsets")))
+			break;
+		const uint32_t grid = grid_for(c, T, SUP_THREADS / 32, 32);
+		k_clique_own<<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, T, inc.off, inc.third, inc.tri, own);
+		c.launches++;
+		if ((rc = scan_u32(c, own, qoff, T)))
+			break;
+		uint64_t Q = 0;
+		if (cudaMemcpyAsync(&Q, qoff + T, 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "clique count");
+			break;
+		}
+		if (Q > 0xffffffffull)
+		{
+			rc = fail(NUCLEUS34_E_RANGE32, "four-clique count " + std::to_string(Q) +
+											   " exceeds the 32-bit clique id range of the direct variant; "
+											   "use the on-demand variant");
+			break;
+		}
+		c.Q = Q;
+		c.release(own);
+		own = nullptr;
+		if (Q == 0)
+			break;
+		if ((rc = dalloc(c, &c.dquds, 4 * Q, "four-cliques")))
+			break;
+		k_clique_write<<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, T, inc.off, inc.third, inc.tri, qoff,
+														   reinterpret_cast<uint4 *>(c.dquds));
+		c.launches++;
+		c.release(qoff);
+		qoff = nullptr;
+		// triangle -> clique CSR: counts are the supports
+		if ((rc = dalloc(c, &csr.off, T + 1, "clique csr offsets")))
+			break;
+		static_assert(sizeof(int32_t) == sizeof(uint32_t), "support layout");
+		if ((rc = scan_u32(c, reinterpret_cast<const uint32_t *>(support), csr.off, T)))
+			break;
+		if ((rc = dalloc(c, &csr.ids, 4 * Q, "clique csr ids")))
+			break;
+		if ((rc = dalloc(c, &cursor, T, "clique csr cursor")))
+			break;
+		if ((rc = dalloc(c, &errf, 1, "clique check")))
+			break;
+		if (cudaMemsetAsync(cursor, 0, T * 4, c.stream) != cudaSuccess ||
+			cudaMemsetAsync(errf, 0, 4, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "memset");
+			break;
+		}
+		k_clique_fill<<<grid_for(c, Q, 256), 256, 0, c.stream>>>(reinterpret_cast<const uint4 *>(c.dquds), Q,
+																  csr.off, cursor, csr.ids, errf);
+		c.launches++;
+		uint32_t herr = 0;
+		if (cudaGetLastError() != cudaSuccess ||
+			cudaMemcpyAsync(&herr, errf, 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+			rc = fail(NUCLEUS34_E_CUDA, "clique kernels");
+		else if (herr)
+			rc = fail(NUCLEUS34_E_CUDA, "internal: clique incidence overflow");
+	} while (false);
+	cleanup();
+	return rc;
+}
+
+void free_clique_csr(Ctx &c, CliqueCsr &csr)
+{
+	c.release(csr.off);
+	c.release(csr.ids);
+	csr = CliqueCsr{};
+}
+
+} // namespace n34

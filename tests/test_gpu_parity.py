@@ -1,0 +1,100 @@
+"""Parity of the CUDA path (through the C-ABI) with the CPU oracle.
+
+Bit-exact: triangle list (canonical (a,b) order), triangle count, four-clique
+count, every triangle's k, K_max and K_avg, for both variants."""
+import numpy as np
+import pytest
+
+import graphs
+
+pytestmark = pytest.mark.gpu
+
+VARIANTS = ["direct", "ondemand"]
+
+
+def check_against_oracle(n34, oracle, g, variant):
+    d = n34.decompose(g, variant=variant, n_quds=5)
+    o = oracle.decompose(g, quds_cap=5)
+    r = d.result
+    assert r["triangle_count"] == o.T
+    assert r["four_clique_count"] == o.Q
+    assert d.tris.shape == o.tris.shape
+    assert np.array_equal(d.tris, o.tris), "canonical triangle list differs"
+    assert np.array_equal(d.k, o.k), "per-triangle k differs"
+    if o.Q:
+        assert r["k_max"] == o.k_max
+        assert r["k_avg"] == o.k_avg
+        assert r["unpeeled_count"] == 0
+    if variant == "direct" and o.Q:
+        assert np.array_equal(d.quds, o.quds[: len(d.quds)])
+    return d, o
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("name", sorted(graphs.SMALL))
+def test_small_known_graphs(n34, oracle, name, variant):
+    s, t = graphs.SMALL[name]()
+    g = n34.graph_from_edges(s, t)
+    d, o = check_against_oracle(n34, oracle, g, variant)
+    if name.startswith("K") and "_" not in name:
+        n = int(name[1:])
+        assert d.result["four_clique_count"] == n * (n - 1) * (n - 2) * (n - 3) // 24
+        assert np.all(d.k == n - 3)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_c1_rmat12(n34, oracle, variant):
+    """R-MAT scale 12, edge factor 16, seed 1 (the plain small configuration)."""
+    s, t = n34.gen_rmat(12, 16, 1)
+    g = n34.graph_from_edges(s, t)
+    d, o = check_against_oracle(n34, oracle, g, variant)
+    assert o.T > 400_000 and o.Q > 3_000_000
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("case", [("rmat", 10, 8, 7), ("rmat", 13, 24, 99), ("ws", 5000, 10, 3),
+                                  ("rgg", 30000, 32, 5)])
+def test_random_graphs(n34, oracle, variant, case):
+    kind = case[0]
+    if kind == "rmat":
+        s, t = n34.gen_rmat(case[1], case[2], case[3])
+    elif kind == "ws":
+        s, t = n34.gen_ws(case[1], case[2], 0.1, case[3])
+    else:
+        s, t = n34.gen_rgg(case[1], case[2], case[3])
+    g = n34.graph_from_edges(s, t)
+    check_against_oracle(n34, oracle, g, variant)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_no_triangles_and_empty(n34, oracle, variant):
+    for s, t in [graphs.triangle_free(), (np.array([0], np.uint32), np.array([1], np.uint32))]:
+        g = n34.graph_from_edges(s, t)
+        d = n34.decompose(g, variant=variant)
+        assert d.result["triangle_count"] == 0
+        assert d.result["four_clique_count"] == 0
+        assert len(d.k) == 0
+
+
+def test_context_reuse_is_deterministic(n34):
+    s, t = n34.gen_rmat(11, 16, 5)
+    g = n34.graph_from_edges(s, t)
+    with n34.Context() as ctx:
+        ctx.upload(g)
+        outs = []
+        for v in ["ondemand", "direct", "ondemand"]:
+            r = ctx.run(v)
+            k, tris = ctx.copy_k(r["triangle_count"], with_tris=True)
+            outs.append((r["four_clique_count"], k, tris))
+    for q, k, tris in outs[1:]:
+        assert q == outs[0][0]
+        assert np.array_equal(k, outs[0][1])
+        assert np.array_equal(tris, outs[0][2])
+
+
+def test_budget_exceeded_is_reported(n34):
+    s, t = n34.gen_rmat(12, 16, 1)
+    g = n34.graph_from_edges(s, t)
+    with pytest.raises(n34.Nucleus34Error) as ei:
+        n34.decompose(g, variant="direct", mem_budget_bytes=1 << 20)
+    assert ei.value.code == n34.E_OOM_BUDGET
