@@ -221,6 +221,7 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 	Incidence inc;
 	CliqueCsr csr;
 	int32_t *S = nullptr;
+	uint32_t *own = nullptr;
 	int rc = NUCLEUS34_OK;
 	PeelCtl pc{};
 	bool peeled = false;
@@ -236,6 +237,7 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 		{
 			if ((rc = build_incidence(c, inc)))
 				break;
+			r.sum_te_sq = inc.sum_te_sq;
 		}
 		N34_CUDA(cudaEventRecord(ev.e[2], c.stream));
 		uint64_t total = 0;
@@ -243,7 +245,9 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 		{
 			if ((rc = dalloc(c, &S, c.T, "support")))
 				break;
-			if ((rc = count_support(c, inc, S, &total)))
+			if (variant == NUCLEUS34_DIRECT && (rc = dalloc(c, &own, c.T, "clique owner counts")))
+				break;
+			if ((rc = count_support(c, inc, S, &total, own)))
 				break;
 			if (total % 4)
 			{
@@ -255,7 +259,7 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 		N34_CUDA(cudaEventRecord(ev.e[3], c.stream));
 		if (variant == NUCLEUS34_DIRECT && total)
 		{
-			if ((rc = list_cliques(c, inc, S, csr)))
+			if ((rc = list_cliques(c, inc, S, own, csr)))
 				break;
 			if (c.Q != total / 4)
 			{
@@ -263,6 +267,8 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 				break;
 			}
 		}
+		c.release(own);
+		own = nullptr;
 		if (variant == NUCLEUS34_DIRECT)
 			free_incidence(c, inc);
 		N34_CUDA(cudaEventRecord(ev.e[4], c.stream));
@@ -287,6 +293,7 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 	free_incidence(c, inc);
 	free_clique_csr(c, csr);
 	c.release(S);
+	c.release(own);
 	if (rc)
 	{
 		c.release_results();
@@ -394,11 +401,24 @@ int create_ctx(const nucleus34_opts *opts, nucleus34_ctx *out)
 		delete x;
 		return fail(NUCLEUS34_E_CUDA, "stream creation");
 	}
+	// Keep freed blocks mapped in the stream-ordered pool between phases and
+	// runs: re-mapping tens of GB costs far more than the kernels themselves.
+	{
+		cudaMemPool_t pool;
+		if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess)
+		{
+			uint64_t thr = UINT64_MAX;
+			cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+		}
+		cudaGetLastError();
+	}
 	size_t fb = 0, tb = 0;
 	cudaMemGetInfo(&fb, &tb);
 	c.budget = (opts && opts->mem_budget_bytes) ? opts->mem_budget_bytes : uint64_t(double(fb) * 0.9);
 	if (opts && opts->tune_table)
 		c.tune_table = opts->tune_table;
+	if (opts)
+		c.opt_flags = opts->flags;
 	*out = x;
 	return NUCLEUS34_OK;
 }
@@ -418,6 +438,12 @@ void destroy_ctx(nucleus34_ctx x)
 	{
 		cudaStreamSynchronize(c.stream);
 		cudaStreamDestroy(c.stream);
+	}
+	{
+		cudaMemPool_t pool;
+		if (cudaDeviceGetDefaultMemPool(&pool, c.device) == cudaSuccess)
+			cudaMemPoolTrimTo(pool, 0);
+		cudaGetLastError();
 	}
 	delete x;
 }

@@ -80,6 +80,7 @@ struct Ctx
 	uint64_t peak = 0;
 	uint64_t launches = 0;
 	std::string tune_table;
+	uint32_t opt_flags = 0;
 	std::mutex mu;
 
 	// resident graph

@@ -193,6 +193,22 @@ __global__ void __launch_bounds__(SEG_BLOCK) k_seg_sort_global(const uint32_t *_
 	}
 }
 
+__global__ void k_sum_sq(const uint64_t *__restrict__ off, uint64_t m, unsigned long long *__restrict__ out)
+{
+	unsigned long long acc = 0;
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t e = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < m; e += stride)
+	{
+		const unsigned long long d = off[e + 1] - off[e];
+		acc += d * d;
+	}
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		acc += __shfl_xor_sync(FULL, acc, o);
+	if (lane_id() == 0 && acc)
+		atomicAdd(out, acc);
+}
+
 __global__ void k_inc_split(const unsigned long long *__restrict__ keys, uint64_t n, uint32_t *__restrict__ third,
 							uint32_t *__restrict__ tri)
 {
@@ -211,7 +227,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 {
 	const uint64_t T = c.T, m = c.m, n3 = 3 * T;
 	uint32_t *cnt = nullptr, *lists = nullptr, *counts = nullptr, *errf = nullptr;
-	unsigned long long *keys = nullptr, *scratch = nullptr, *maxlen = nullptr;
+	unsigned long long *keys = nullptr, *scratch = nullptr, *maxlen = nullptr, *sumsq = nullptr;
 	int rc = NUCLEUS34_OK;
 	auto cleanup = [&] {
 		c.release(cnt);
@@ -221,6 +237,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 		c.release(scratch);
 		c.release(maxlen);
 		c.release(errf);
+		c.release(sumsq);
 	};
 	do
 	{
@@ -262,18 +279,24 @@ int build_incidence(Ctx &c, Incidence &inc)
 			break;
 		if ((rc = dalloc(c, &maxlen, 1, "segment max")))
 			break;
+		if ((rc = dalloc(c, &sumsq, 1, "segment square sum")))
+			break;
 		if (cudaMemsetAsync(counts, 0, 16, c.stream) != cudaSuccess ||
-			cudaMemsetAsync(maxlen, 0, 8, c.stream) != cudaSuccess)
+			cudaMemsetAsync(maxlen, 0, 8, c.stream) != cudaSuccess ||
+			cudaMemsetAsync(sumsq, 0, 8, c.stream) != cudaSuccess)
 		{
 			rc = fail(NUCLEUS34_E_CUDA, "memset");
 			break;
 		}
 		k_seg_classify<<<grid_for(c, m, 256), 256, 0, c.stream>>>(inc.off, m, lists, counts, m, maxlen);
 		c.launches++;
+		k_sum_sq<<<grid_for(c, m, 256), 256, 0, c.stream>>>(inc.off, m, sumsq);
+		c.launches++;
 		uint32_t hcounts[4] = {0, 0, 0, 0};
 		unsigned long long hmax = 0;
 		uint32_t herr = 0;
-		if (cudaMemcpyAsync(&herr, errf, 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+		if (cudaMemcpyAsync(&inc.sum_te_sq, sumsq, 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaMemcpyAsync(&herr, errf, 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
 			cudaMemcpyAsync(hcounts, counts, 16, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
 			cudaMemcpyAsync(&hmax, maxlen, 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
 			cudaStreamSynchronize(c.stream) != cudaSuccess)

@@ -59,4 +59,57 @@ __device__ __forceinline__ void warp_intersect3(const uint32_t *__restrict__ thi
 	}
 }
 
+// The shortest of the three lists drives; the other two are searched.
+struct Driver
+{
+	uint64_t bd, ed, lo1, hi1, lo2, hi2;
+};
+
+__device__ __forceinline__ Driver pick_driver(uint64_t b0, uint64_t e0, uint64_t b1, uint64_t e1, uint64_t b2,
+											  uint64_t e2)
+{
+	Driver d{b0, e0, b1, e1, b2, e2};
+	if (e1 - b1 < d.ed - d.bd)
+	{
+		d.bd = b1;
+		d.ed = e1;
+		d.lo1 = b0;
+		d.hi1 = e0;
+	}
+	if (e2 - b2 < d.ed - d.bd)
+	{
+		d.lo2 = d.bd;
+		d.hi2 = d.ed;
+		d.bd = b2;
+		d.ed = e2;
+	}
+	return d;
+}
+
+// Driver length up to which one lane handles a triangle on its own (the
+// lanes of a warp then work on 32 different triangles at once).
+constexpr uint64_t THREAD_MODE_MAX = 16;
+
+// Thread-local 3-way intersection for a short driver list: f(x, pd, p1, p2)
+// per common third. Windows only move forward because the driver is sorted.
+template <class F>
+__device__ __forceinline__ void thread_intersect3(const uint32_t *__restrict__ third, Driver d, F &&f)
+{
+	for (uint64_t i = d.bd; i < d.ed && d.lo1 < d.hi1 && d.lo2 < d.hi2; ++i)
+	{
+		const uint32_t x = __ldg(third + i);
+		d.lo1 = lower_bound_u32(third, d.lo1, d.hi1, x);
+		if (d.lo1 >= d.hi1)
+			break;
+		if (__ldg(third + d.lo1) != x)
+			continue;
+		d.lo2 = lower_bound_u32(third, d.lo2, d.hi2, x);
+		if (d.lo2 >= d.hi2)
+			break;
+		if (__ldg(third + d.lo2) != x)
+			continue;
+		f(x, i, d.lo1, d.lo2);
+	}
+}
+
 } // namespace n34

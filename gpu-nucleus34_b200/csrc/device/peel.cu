@@ -50,24 +50,50 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
 	{
 		PeelCtl z{};
 		z.minS = INF;
+		z.level = 0xffffffffu; // "-1": the first level change tries level 0
 		ctl->c = z;
 		ctl->scan = 1;
 	}
 }
 
-__global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int32_t *__restrict__ S,
-														   const int32_t *__restrict__ K, uint64_t T)
+// Level change (frontier empty): every alive triangle has S > level, and dead
+// ones hold S = INT_MAX. First try the next level directly (the usual case);
+// only if nothing sits at level+1 compute the minimum and gather at it.
+__global__ void __launch_bounds__(PEEL_THREADS) k_gather_next(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T,
+															  uint32_t *__restrict__ F0, uint32_t *__restrict__ F1)
 {
 	if (ctl->c.done || !ctl->scan)
+		return;
+	const int32_t want = int32_t(ctl->c.level) + 1;
+	uint32_t *F = ctl->c.cur ? F1 : F0;
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < T; t0 += stride)
+	{
+		const uint64_t t = t0 + threadIdx.x;
+		const bool take = t < T && S[t] <= want;
+		const uint32_t slot = warp_append(take, &ctl->c.nF);
+		if (take)
+		{
+			if (slot < T)
+				F[slot] = uint32_t(t);
+			else
+				atomicOr(&ctl->c.error, 1u);
+		}
+	}
+}
+
+__global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T)
+{
+	if (ctl->c.done || !ctl->scan || ctl->c.nF)
 		return;
 	uint32_t mn = INF;
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
-		if (K[t] == -1)
-		{
-			const int32_t s = S[t];
+	{
+		const int32_t s = S[t];
+		if (s != INT32_MAX)
 			mn = min(mn, uint32_t(s < 0 ? 0 : s));
-		}
+	}
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1)
 		mn = min(mn, __shfl_xor_sync(FULL, mn, o));
@@ -75,12 +101,18 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int3
 		atomicMin(&ctl->c.minS, mn);
 }
 
-__global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_t *__restrict__ S,
-														 const int32_t *__restrict__ K, uint64_t T,
+// Second chance of the level change: gather at the minimum (or finish).
+__global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T,
 														 uint32_t *__restrict__ F0, uint32_t *__restrict__ F1)
 {
 	if (ctl->c.done || !ctl->scan)
 		return;
+	if (ctl->c.nF)
+	{ // k_gather_next found the frontier at level+1
+		if (blockIdx.x == 0 && threadIdx.x == 0)
+			ctl->c.level = ctl->c.level + 1;
+		return;
+	}
 	const uint32_t mn = ctl->c.minS;
 	if (mn == INF)
 	{
@@ -88,18 +120,19 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_
 			ctl->c.done = 1;
 		return;
 	}
+	// every alive triangle sits above the old level, so the minimum is the new one
 	if (blockIdx.x == 0 && threadIdx.x == 0)
-		ctl->c.level = max(ctl->c.level, mn);
+		ctl->c.level = mn;
 	uint32_t *F = ctl->c.cur ? F1 : F0;
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < T; t0 += stride)
 	{
 		const uint64_t t = t0 + threadIdx.x;
 		bool take = false;
-		if (t < T && K[t] == -1)
+		if (t < T)
 		{
 			const int32_t s = S[t];
-			take = uint32_t(s < 0 ? 0 : s) <= mn;
+			take = s != INT32_MAX && uint32_t(s < 0 ? 0 : s) <= mn;
 		}
 		const uint32_t slot = warp_append(take, &ctl->c.nF);
 		if (take)
@@ -113,7 +146,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_
 }
 
 __global__ void k_mark(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
-					   int32_t *__restrict__ K, uint32_t *__restrict__ R)
+					   int32_t *__restrict__ K, uint32_t *__restrict__ R, int32_t *__restrict__ S)
 {
 	if (ctl->c.done)
 		return;
@@ -127,6 +160,7 @@ __global__ void k_mark(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_
 		const uint32_t t = F[i];
 		K[t] = level;
 		R[t] = round;
+		S[t] = INT32_MAX; // dead: out of every later scan (dead triangles are never debited)
 	}
 }
 
@@ -226,10 +260,14 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_ondemand(
 	}
 }
 
+// Direct variant: a dying triangle walks its clique ids. A clique destroyed in
+// an earlier round carries a set byte in `destroyed` (written by its owner), so
+// later members skip it with one byte load; otherwise the members are read and
+// the round-stamp owner rule decides.
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_direct(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint64_t *__restrict__ coff,
 	const uint32_t *__restrict__ cids, const uint4 *__restrict__ quds, const int32_t *__restrict__ K,
-	const uint32_t *__restrict__ R, int32_t *__restrict__ S, uint64_t T)
+	const uint32_t *__restrict__ R, int32_t *__restrict__ S, uint8_t *__restrict__ destroyed, uint64_t T)
 {
 	if (ctl->c.done)
 		return;
@@ -247,14 +285,19 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_direct(
 		for (uint64_t base = b; base < e; base += 32)
 		{
 			const uint64_t j = base + lane_id();
-			const bool found = j < e;
-			uint32_t q0 = 0, q1 = 0, q2 = 0;
-			if (found)
+			bool live = false;
+			uint32_t q = 0, q0 = 0, q1 = 0, q2 = 0;
+			if (j < e)
 			{
-				const uint4 q = quds[cids[j]];
+				q = cids[j];
+				live = !destroyed[q];
+			}
+			if (live)
+			{
+				const uint4 x = quds[q];
 				// the three members other than t
-				const uint32_t m[4] = {q.x, q.y, q.z, q.w};
-				uint32_t o[3];
+				const uint32_t m[4] = {x.x, x.y, x.z, x.w};
+				uint32_t o[3] = {0, 0, 0};
 				int k = 0;
 #pragma unroll
 				for (int s = 0; s < 4; ++s)
@@ -264,7 +307,276 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_direct(
 				q1 = o[1];
 				q2 = o[2];
 			}
-			settle_clique(found, t, q0, q1, q2, K, R, S, round, level, Fn, &ctl->c.nNext, T, &ctl->c.error);
+			bool owner = live;
+			bool al[3] = {false, false, false};
+			if (live)
+			{
+				const uint32_t p[3] = {q0, q1, q2};
+#pragma unroll
+				for (int s = 0; s < 3; ++s)
+				{
+					al[s] = K[p[s]] == -1;
+					if (!al[s] && (R[p[s]] < round || p[s] < t))
+						owner = false;
+				}
+			}
+			bool hit[3] = {false, false, false};
+			if (owner)
+			{
+				destroyed[q] = 1;
+				if (al[0])
+					hit[0] = atomicSub(S + q0, 1) == level + 1;
+				if (al[1])
+					hit[1] = atomicSub(S + q1, 1) == level + 1;
+				if (al[2])
+					hit[2] = atomicSub(S + q2, 1) == level + 1;
+			}
+			const uint32_t qs[3] = {q0, q1, q2};
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+			{
+				const uint32_t slot = warp_append(hit[r], &ctl->c.nNext);
+				if (hit[r])
+				{
+					if (slot < T)
+						Fn[slot] = qs[r];
+					else
+						atomicOr(&ctl->c.error, 1u);
+				}
+			}
+		}
+	}
+}
+
+// ---- on-demand peel with death flags kept in the incidence entries ----------
+//
+// Each triangle owns one entry in each of its three edges' lists; bit 31 of the
+// entry's triangle id means "died in an earlier round", bit 30 "dies in this
+// round". The owner rule then reads nothing but the three entries the 3-way
+// intersection already located, and a dead driver entry skips its searches.
+constexpr uint32_t DEAD = 0x80000000u;
+constexpr uint32_t DYING = 0x40000000u;
+constexpr uint32_t ID_MASK = 0x3fffffffu;
+
+// positions of triangle t's three entries: under b (third w), a (third v), c (third u)
+__device__ __forceinline__ void entry_positions(uint32_t t, const uint32_t *__restrict__ tris,
+												const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
+												const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third,
+												uint64_t pos[3])
+{
+	const uint32_t a = __ldg(tris + 3 * uint64_t(t)), b = __ldg(tris + 3 * uint64_t(t) + 1),
+				   c = __ldg(tris + 3 * uint64_t(t) + 2);
+	const uint32_t u = __ldg(src + b), v = __ldg(E + b), w = __ldg(E + c);
+	pos[0] = lower_bound_u32(third, incO[b], incO[b + 1], w);
+	pos[1] = lower_bound_u32(third, incO[a], incO[a + 1], v);
+	pos[2] = lower_bound_u32(third, incO[c], incO[c + 1], u);
+}
+
+__global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
+							 int32_t *__restrict__ K, int32_t *__restrict__ S, const uint32_t *__restrict__ tris,
+							 const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
+							 const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third,
+							 uint32_t *__restrict__ itri, uint64_t n3)
+{
+	if (ctl->c.done)
+		return;
+	const uint32_t nF = ctl->c.nF;
+	const uint32_t *F = ctl->c.cur ? F1 : F0;
+	const int32_t level = int32_t(ctl->c.level);
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nF; i += stride)
+	{
+		const uint32_t t = F[i];
+		K[t] = level;
+		S[t] = INT32_MAX;
+		uint64_t pos[3];
+		entry_positions(t, tris, src, E, incO, third, pos);
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+			if (pos[r] < n3)
+				itri[pos[r]] = t | DYING;
+	}
+}
+
+__global__ void k_finalize_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
+								 const uint32_t *__restrict__ tris, const uint32_t *__restrict__ src,
+								 const uint32_t *__restrict__ E, const uint64_t *__restrict__ incO,
+								 const uint32_t *__restrict__ third, uint32_t *__restrict__ itri, uint64_t n3)
+{
+	if (ctl->c.done)
+		return;
+	const uint32_t nF = ctl->c.nF;
+	const uint32_t *F = ctl->c.cur ? F1 : F0;
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nF; i += stride)
+	{
+		const uint32_t t = F[i];
+		uint64_t pos[3];
+		entry_positions(t, tris, src, E, incO, third, pos);
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+			if (pos[r] < n3)
+				itri[pos[r]] = t | DEAD;
+	}
+}
+
+// Owner rule on flagged entries: q0..q2 are the three partners' entries (no
+// DEAD bit); t owns the clique unless a partner dying this round has a
+// smaller id. Returns which partners crossed level+1 -> level.
+__device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q1, uint32_t q2,
+											 int32_t *__restrict__ S, int32_t level, bool hit[3])
+{
+	hit[0] = hit[1] = hit[2] = false;
+	if (((q0 & DYING) && (q0 & ID_MASK) < t) || ((q1 & DYING) && (q1 & ID_MASK) < t) ||
+		((q2 & DYING) && (q2 & ID_MASK) < t))
+		return;
+	if (!(q0 & DYING))
+		hit[0] = atomicSub(S + q0, 1) == level + 1;
+	if (!(q1 & DYING))
+		hit[1] = atomicSub(S + q1, 1) == level + 1;
+	if (!(q2 & DYING))
+		hit[2] = atomicSub(S + q2, 1) == level + 1;
+}
+
+// Debit of the dying triangles, hybrid like k_support: each warp takes 32
+// frontier entries; short drivers are intersected by their own lane, long ones
+// by the whole warp. Dead driver entries skip their searches.
+__global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags(
+	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
+	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
+	int32_t *__restrict__ S, uint64_t T)
+{
+	if (ctl->c.done)
+		return;
+	const uint32_t nF = ctl->c.nF;
+	const uint32_t *F = ctl->c.cur ? F1 : F0;
+	uint32_t *Fn = ctl->c.cur ? F0 : F1;
+	const int32_t level = int32_t(ctl->c.level);
+	uint32_t *nNext = &ctl->c.nNext;
+	uint32_t *err = &ctl->c.error;
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	const uint32_t lane = lane_id();
+	for (uint64_t base = warp * 32; base < nF; base += nwarps * 32)
+	{
+		const uint64_t fi = base + lane;
+		const bool valid = fi < nF;
+		uint32_t t = 0;
+		Driver d{};
+		if (valid)
+		{
+			t = F[fi];
+			const uint32_t ea = __ldg(tris + 3 * uint64_t(t)), eb = __ldg(tris + 3 * uint64_t(t) + 1),
+						   ec = __ldg(tris + 3 * uint64_t(t) + 2);
+			d = pick_driver(incO[ea], incO[ea + 1], incO[eb], incO[eb + 1], incO[ec], incO[ec + 1]);
+		}
+		const bool small = valid && d.ed - d.bd <= THREAD_MODE_MAX;
+		if (small)
+		{
+			uint64_t lo1 = d.lo1, lo2 = d.lo2;
+			for (uint64_t i = d.bd; i < d.ed && lo1 < d.hi1 && lo2 < d.hi2; ++i)
+			{
+				const uint32_t q0 = itri[i];
+				if (q0 & DEAD)
+					continue;
+				const uint32_t x = __ldg(third + i);
+				lo1 = lower_bound_u32(third, lo1, d.hi1, x);
+				if (lo1 >= d.hi1)
+					break;
+				if (__ldg(third + lo1) != x)
+					continue;
+				const uint32_t q1 = itri[lo1];
+				if (q1 & DEAD)
+					continue;
+				lo2 = lower_bound_u32(third, lo2, d.hi2, x);
+				if (lo2 >= d.hi2)
+					break;
+				if (__ldg(third + lo2) != x)
+					continue;
+				const uint32_t q2 = itri[lo2];
+				if (q2 & DEAD)
+					continue;
+				bool hit[3];
+				settle_flags(t, q0, q1, q2, S, level, hit);
+				const uint32_t qs[3] = {q0, q1, q2};
+#pragma unroll
+				for (int r = 0; r < 3; ++r)
+					if (hit[r])
+					{
+						const uint32_t slot = atomicAdd(nNext, 1u);
+						if (slot < T)
+							Fn[slot] = qs[r];
+						else
+							atomicOr(err, 1u);
+					}
+			}
+		}
+		uint32_t large = __ballot_sync(FULL, valid && !small);
+		while (large)
+		{
+			const int j = __ffs(large) - 1;
+			large &= large - 1;
+			const uint32_t tj = __shfl_sync(FULL, t, j);
+			const uint64_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
+			uint64_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
+			uint64_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
+			for (uint64_t cb = bd; cb < ed; cb += 32)
+			{
+				if (lo1 >= hi1 || lo2 >= hi2)
+					break; // warp-uniform
+				const uint64_t i = cb + lane;
+				const bool iv = i < ed;
+				uint32_t x = 0xffffffffu, q0 = DEAD, q1 = 0, q2 = 0;
+				if (iv)
+				{
+					x = __ldg(third + i);
+					q0 = itri[i];
+				}
+				uint64_t p1 = hi1, p2 = hi2;
+				bool s2 = false, found = false;
+				const bool s1 = iv && !(q0 & DEAD);
+				if (s1)
+				{
+					p1 = lower_bound_u32(third, lo1, hi1, x);
+					if (p1 < hi1 && __ldg(third + p1) == x)
+					{
+						q1 = itri[p1];
+						if (!(q1 & DEAD))
+						{
+							s2 = true;
+							p2 = lower_bound_u32(third, lo2, hi2, x);
+							if (p2 < hi2 && __ldg(third + p2) == x)
+							{
+								q2 = itri[p2];
+								found = !(q2 & DEAD);
+							}
+						}
+					}
+				}
+				// later chunks hold larger x: the highest searching lane's
+				// lower bound stays valid for each list
+				const uint32_t m1 = __ballot_sync(FULL, s1), m2 = __ballot_sync(FULL, s2);
+				if (m1)
+					lo1 = __shfl_sync(FULL, p1, 31 - __clz(m1));
+				if (m2)
+					lo2 = __shfl_sync(FULL, p2, 31 - __clz(m2));
+				bool hit[3] = {false, false, false};
+				if (found)
+					settle_flags(tj, q0, q1, q2, S, level, hit);
+				const uint32_t qs[3] = {q0, q1, q2};
+#pragma unroll
+				for (int r = 0; r < 3; ++r)
+				{
+					const uint32_t slot = warp_append(hit[r], nNext);
+					if (hit[r])
+					{
+						if (slot < T)
+							Fn[slot] = qs[r];
+						else
+							atomicOr(err, 1u);
+					}
+				}
+			}
 		}
 	}
 }
@@ -327,6 +639,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 {
 	const uint64_t T = c.T;
 	uint32_t *R = nullptr, *F0 = nullptr, *F1 = nullptr;
+	uint8_t *destroyed = nullptr;
 	CtlX *ctl = nullptr;
 	int rc = NUCLEUS34_OK;
 	auto cleanup = [&] {
@@ -334,6 +647,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		c.release(F0);
 		c.release(F1);
 		c.release(ctl);
+		c.release(destroyed);
 	};
 	do
 	{
@@ -345,33 +659,86 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			break;
 		if ((rc = dalloc(c, &ctl, 1, "peel control")))
 			break;
+		if (variant == NUCLEUS34_DIRECT)
+		{
+			if ((rc = dalloc(c, &destroyed, c.Q ? c.Q : 1, "clique destroyed flags")))
+				break;
+			if (cudaMemsetAsync(destroyed, 0, c.Q ? c.Q : 1, c.stream) != cudaSuccess)
+			{
+				rc = fail(NUCLEUS34_E_CUDA, "memset");
+				break;
+			}
+		}
+		// death flags live in the incidence entries when triangle ids leave the
+		// top two bits free (the incidence is discarded after the peel)
+		const bool flags =
+			variant == NUCLEUS34_ONDEMAND && T <= ID_MASK && !(c.opt_flags & NUCLEUS34_OPT_STAMP_PEEL);
 		const uint32_t gscan = grid_for(c, T, PEEL_THREADS, 8);
 		const uint32_t gwarp = grid_for(c, T, PEEL_THREADS / 32, 16);
 		k_peel_init<<<gscan, PEEL_THREADS, 0, c.stream>>>(K, T, ctl);
 		c.launches++;
-		// Bounded host loop: at most one peel per triangle per round and each
-		// level costs at least one round, so T + levels + a margin bounds it.
-		const uint64_t max_rounds = 2 * T + 4096;
-		uint64_t rounds = 0;
-		uint32_t batch = 4;
-		bool done = false;
-		while (!done)
-		{
-			for (uint32_t r = 0; r < batch; ++r)
+		// One round = a fixed kernel sequence that reads its sizes from ctl.
+		auto launch_round = [&]() {
+			k_gather_next<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, F0, F1);
+			k_scan_min<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T);
+			k_gather<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, F0, F1);
+			if (flags)
 			{
-				k_scan_min<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, K, T);
-				k_gather<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, K, T, F0, F1);
-				k_mark<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, R);
+				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.off,
+																   inc.third, inc.tri, 3 * T);
+				k_debit_flags<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off, inc.third,
+																	inc.tri, S, T);
+				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, c.dsrc, c.dE, inc.off,
+																	   inc.third, inc.tri, 3 * T);
+			}
+			else
+			{
+				k_mark<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, R, S);
 				if (variant == NUCLEUS34_ONDEMAND)
 					k_debit_ondemand<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off, inc.third,
 																		   inc.tri, K, R, S, T);
 				else
 					k_debit_direct<<<gwarp, PEEL_THREADS, 0, c.stream>>>(
-						ctl, F0, F1, csr.off, csr.ids, reinterpret_cast<const uint4 *>(c.dquds), K, R, S, T);
-				k_advance<<<1, 1, 0, c.stream>>>(ctl);
-				c.launches += 5;
+						ctl, F0, F1, csr.off, csr.ids, reinterpret_cast<const uint4 *>(c.dquds), K, R, S, destroyed,
+						T);
 			}
-			rounds += batch;
+			k_advance<<<1, 1, 0, c.stream>>>(ctl);
+		};
+		const uint32_t per_round = flags ? 7u : 6u;
+		// Rounds are replayed from a CUDA graph of ROUNDS_PER_GRAPH rounds; the
+		// host reads one flag per replay. Rounds after the last one are no-ops.
+		constexpr uint32_t ROUNDS_PER_GRAPH = 16;
+		cudaGraph_t graph = nullptr;
+		cudaGraphExec_t exec = nullptr;
+		bool use_graph = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+		if (use_graph)
+		{
+			for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
+				launch_round();
+			use_graph = cudaStreamEndCapture(c.stream, &graph) == cudaSuccess && graph &&
+						cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+		}
+		cudaGetLastError();
+		// Bounded host loop: every round that is not a no-op peels at least one
+		// triangle, so T + 1 rounds suffice; the bound leaves a wide margin.
+		const uint64_t max_rounds = 2 * T + 4096;
+		uint64_t rounds = 0;
+		bool done = false;
+		while (!done)
+		{
+			if (use_graph)
+			{
+				if (cudaGraphLaunch(exec, c.stream) != cudaSuccess)
+				{
+					rc = fail(NUCLEUS34_E_CUDA, "peel graph launch");
+					break;
+				}
+			}
+			else
+				for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
+					launch_round();
+			rounds += ROUNDS_PER_GRAPH;
+			c.launches += uint64_t(ROUNDS_PER_GRAPH) * per_round;
 			uint32_t hdone = 0;
 			if (cudaGetLastError() != cudaSuccess ||
 				cudaMemcpyAsync(&hdone, &ctl->c.done, 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
@@ -386,9 +753,11 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				rc = fail(NUCLEUS34_E_TIMEOUT, "peel did not converge within its round bound");
 				break;
 			}
-			if (batch < 64)
-				batch *= 2;
 		}
+		if (exec)
+			cudaGraphExecDestroy(exec);
+		if (graph)
+			cudaGraphDestroy(graph);
 		if (rc)
 			break;
 		k_stats<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, K, T);

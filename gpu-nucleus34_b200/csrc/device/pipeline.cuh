@@ -11,6 +11,7 @@ struct Incidence
 	uint64_t *off = nullptr;   // m+1
 	uint32_t *third = nullptr; // 3T
 	uint32_t *tri = nullptr;   // 3T
+	unsigned long long sum_te_sq = 0; // sum over edges of (list length)^2
 };
 
 // Triangle -> four-clique incidence of the direct variant.
@@ -25,9 +26,10 @@ int list_triangles(Ctx &c);
 int build_incidence(Ctx &c, Incidence &inc);
 void free_incidence(Ctx &c, Incidence &inc);
 // support[t] = number of four-cliques on t; returns sum(support) in *total.
-int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total);
+// own (optional): cliques whose lowest triangle is t (direct variant sizes).
+int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total, uint32_t *own);
 // Direct variant: canonical clique list (c.dquds, c.Q) and triangle->clique CSR.
-int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, CliqueCsr &csr);
+int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, const uint32_t *own, CliqueCsr &csr);
 void free_clique_csr(Ctx &c, CliqueCsr &csr);
 // Device-resident peel; K receives the final k of every triangle.
 int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_t *support, int32_t *K,

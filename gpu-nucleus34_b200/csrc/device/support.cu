@@ -42,59 +42,83 @@ __device__ __forceinline__ TriEdges tri_lists(const uint32_t *__restrict__ tris,
 	return L;
 }
 
+// Hybrid: each warp takes 32 consecutive triangles, one per lane. Lanes whose
+// shortest list is short intersect on their own; the warp then handles the
+// remaining triangles one at a time with all 32 lanes. With WITH_OWN it also
+// counts the cliques whose lowest triangle id is t (the direct variant's
+// clique-list sizes), from the partner ids the intersection located.
+template <bool WITH_OWN>
 __global__ void __launch_bounds__(SUP_THREADS) k_support(const uint32_t *__restrict__ tris, uint64_t T,
 														 const uint64_t *__restrict__ incO,
 														 const uint32_t *__restrict__ third,
-														 int32_t *__restrict__ support,
+														 const uint32_t *__restrict__ itri,
+														 int32_t *__restrict__ support, uint32_t *__restrict__ own,
 														 unsigned long long *__restrict__ total)
 {
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	const uint32_t lane = lane_id();
 	unsigned long long acc = 0;
-	for (uint64_t t = warp; t < T; t += nwarps)
+	for (uint64_t base = warp * 32; base < T; base += nwarps * 32)
 	{
-		const TriEdges L = tri_lists(tris, incO, t);
-		uint32_t cnt = 0;
-		warp_intersect3(third, L.b0, L.e0, L.b1, L.e1, L.b2, L.e2,
-						[&](bool found, uint32_t, uint64_t, uint64_t, uint64_t) {
-							cnt += __popc(__ballot_sync(FULL, found));
-						});
-		if (lane_id() == 0)
+		const uint64_t t = base + lane;
+		const bool valid = t < T;
+		Driver d{};
+		if (valid)
 		{
+			const TriEdges L = tri_lists(tris, incO, t);
+			d = pick_driver(L.b0, L.e0, L.b1, L.e1, L.b2, L.e2);
+		}
+		const bool small = valid && d.ed - d.bd <= THREAD_MODE_MAX;
+		if (small)
+		{
+			uint32_t cnt = 0, mine = 0;
+			thread_intersect3(third, d, [&](uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+				++cnt;
+				if (WITH_OWN)
+					mine += uint32_t(t) < __ldg(itri + pd) && uint32_t(t) < __ldg(itri + p1) &&
+							uint32_t(t) < __ldg(itri + p2);
+			});
 			support[t] = int32_t(cnt);
+			if (WITH_OWN)
+				own[t] = mine;
 			acc += cnt;
 		}
+		uint32_t large = __ballot_sync(FULL, valid && !small);
+		while (large)
+		{
+			const int j = __ffs(large) - 1;
+			large &= large - 1;
+			const uint64_t tj = base + uint64_t(j);
+			const uint64_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
+			const uint64_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
+			const uint64_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
+			uint32_t cnt = 0, mine = 0;
+			warp_intersect3(third, bd, ed, lo1, hi1, lo2, hi2,
+							[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+								cnt += __popc(__ballot_sync(FULL, found));
+								if (WITH_OWN)
+								{
+									const bool m = found && uint32_t(tj) < __ldg(itri + pd) &&
+												   uint32_t(tj) < __ldg(itri + p1) &&
+												   uint32_t(tj) < __ldg(itri + p2);
+									mine += __popc(__ballot_sync(FULL, m));
+								}
+							});
+			if (lane == uint32_t(j))
+			{
+				support[tj] = int32_t(cnt);
+				if (WITH_OWN)
+					own[tj] = mine;
+				acc += cnt;
+			}
+		}
 	}
-	if (lane_id() == 0 && acc)
+#pragma unroll
+	for (int o = 16; o > 0; o >>= 1)
+		acc += __shfl_xor_sync(FULL, acc, o);
+	if (lane == 0 && acc)
 		atomicAdd(total, acc);
-}
-
-// own[t] = cliques whose lowest triangle is t
-__global__ void __launch_bounds__(SUP_THREADS) k_clique_own(const uint32_t *__restrict__ tris, uint64_t T,
-															const uint64_t *__restrict__ incO,
-															const uint32_t *__restrict__ third,
-															const uint32_t *__restrict__ itri,
-															uint32_t *__restrict__ own)
-{
-	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-	for (uint64_t t = warp; t < T; t += nwarps)
-	{
-		const TriEdges L = tri_lists(tris, incO, t);
-		uint32_t cnt = 0;
-		warp_intersect3(third, L.b0, L.e0, L.b1, L.e1, L.b2, L.e2,
-						[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
-							bool mine = false;
-							if (found)
-							{
-								const uint32_t q0 = __ldg(itri + pd), q1 = __ldg(itri + p1), q2 = __ldg(itri + p2);
-								mine = uint32_t(t) < q0 && uint32_t(t) < q1 && uint32_t(t) < q2;
-							}
-							cnt += __popc(__ballot_sync(FULL, mine));
-						});
-		if (lane_id() == 0)
-			own[t] = cnt;
-	}
 }
 
 __device__ __forceinline__ void sort3(uint32_t &a, uint32_t &b, uint32_t &c)
@@ -120,6 +144,8 @@ __device__ __forceinline__ void sort3(uint32_t &a, uint32_t &b, uint32_t &c)
 	}
 }
 
+// Writes each triangle's owned cliques (lowest member t) at qoff[t], in
+// ascending fourth-vertex order; same hybrid thread/warp split as k_support.
 __global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__restrict__ tris, uint64_t T,
 															  const uint64_t *__restrict__ incO,
 															  const uint32_t *__restrict__ third,
@@ -129,33 +155,68 @@ __global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__
 {
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-	for (uint64_t t = warp; t < T; t += nwarps)
+	const uint32_t lane = lane_id();
+	for (uint64_t base = warp * 32; base < T; base += nwarps * 32)
 	{
-		uint64_t out = qoff[t];
-		const uint64_t out_end = qoff[t + 1];
-		if (out == out_end)
-			continue;
-		const TriEdges L = tri_lists(tris, incO, t);
-		warp_intersect3(third, L.b0, L.e0, L.b1, L.e1, L.b2, L.e2,
-						[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
-							bool mine = false;
-							uint32_t q0 = 0, q1 = 0, q2 = 0;
-							if (found)
-							{
-								q0 = __ldg(itri + pd);
-								q1 = __ldg(itri + p1);
-								q2 = __ldg(itri + p2);
-								mine = uint32_t(t) < q0 && uint32_t(t) < q1 && uint32_t(t) < q2;
-							}
-							const uint32_t word = __ballot_sync(FULL, mine);
-							const uint64_t at = out + __popc(word & lanemask_lt());
-							if (mine && at < out_end) // capacity guard (the count pass sized it)
-							{
-								sort3(q0, q1, q2);
-								quds[at] = make_uint4(uint32_t(t), q0, q1, q2);
-							}
-							out += __popc(word);
-						});
+		const uint64_t t = base + lane;
+		bool work = false;
+		Driver d{};
+		uint64_t out = 0, out_end = 0;
+		if (t < T)
+		{
+			out = qoff[t];
+			out_end = qoff[t + 1];
+			work = out < out_end;
+			if (work)
+			{
+				const TriEdges L = tri_lists(tris, incO, t);
+				d = pick_driver(L.b0, L.e0, L.b1, L.e1, L.b2, L.e2);
+			}
+		}
+		const bool small = work && d.ed - d.bd <= THREAD_MODE_MAX;
+		if (small)
+		{
+			thread_intersect3(third, d, [&](uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+				uint32_t q0 = __ldg(itri + pd), q1 = __ldg(itri + p1), q2 = __ldg(itri + p2);
+				if (uint32_t(t) < q0 && uint32_t(t) < q1 && uint32_t(t) < q2 && out < out_end)
+				{
+					sort3(q0, q1, q2);
+					quds[out++] = make_uint4(uint32_t(t), q0, q1, q2);
+				}
+			});
+		}
+		uint32_t large = __ballot_sync(FULL, work && !small);
+		while (large)
+		{
+			const int j = __ffs(large) - 1;
+			large &= large - 1;
+			const uint32_t tj = uint32_t(base) + uint32_t(j);
+			uint64_t o = __shfl_sync(FULL, out, j);
+			const uint64_t oe = __shfl_sync(FULL, out_end, j);
+			const uint64_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
+			const uint64_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
+			const uint64_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
+			warp_intersect3(third, bd, ed, lo1, hi1, lo2, hi2,
+							[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+								bool mine = false;
+								uint32_t q0 = 0, q1 = 0, q2 = 0;
+								if (found)
+								{
+									q0 = __ldg(itri + pd);
+									q1 = __ldg(itri + p1);
+									q2 = __ldg(itri + p2);
+									mine = tj < q0 && tj < q1 && tj < q2;
+								}
+								const uint32_t word = __ballot_sync(FULL, mine);
+								const uint64_t at = o + __popc(word & lanemask_lt());
+								if (mine && at < oe) // capacity guard (the count pass sized it)
+								{
+									sort3(q0, q1, q2);
+									quds[at] = make_uint4(tj, q0, q1, q2);
+								}
+								o += __popc(word);
+							});
+		}
 	}
 }
 
@@ -182,7 +243,7 @@ __global__ void k_clique_fill(const uint4 *__restrict__ quds, uint64_t Q, const 
 
 } // namespace
 
-int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total)
+int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total, uint32_t *own)
 {
 	unsigned long long *dtot = nullptr;
 	N34_TRY(dalloc(c, &dtot, 1, "support total"));
@@ -194,8 +255,13 @@ int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *tota
 			rc = fail(NUCLEUS34_E_CUDA, "memset");
 			break;
 		}
-		k_support<<<grid_for(c, c.T, SUP_THREADS / 32, 32), SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.off,
-																						 inc.third, support, dtot);
+		const uint32_t grid = grid_for(c, (c.T + 31) / 32, SUP_THREADS / 32, 32);
+		if (own)
+			k_support<true><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.off, inc.third, inc.tri, support,
+																own, dtot);
+		else
+			k_support<false><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.off, inc.third, inc.tri,
+																 support, nullptr, dtot);
 		c.launches++;
 		unsigned long long h = 0;
 		if (cudaGetLastError() != cudaSuccess ||
@@ -211,27 +277,22 @@ int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *tota
 	return rc;
 }
 
-int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, CliqueCsr &csr)
+int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, const uint32_t *own, CliqueCsr &csr)
 {
 	const uint64_t T = c.T;
-	uint32_t *own = nullptr, *cursor = nullptr, *errf = nullptr;
+	uint32_t *cursor = nullptr, *errf = nullptr;
 	uint64_t *qoff = nullptr;
 	int rc = NUCLEUS34_OK;
 	auto cleanup = [&] {
-		c.release(own);
 		c.release(cursor);
 		c.release(qoff);
 		c.release(errf);
 	};
 	do
 	{
-		if ((rc = dalloc(c, &own, T, "clique owner counts")))
-			break;
 		if ((rc = dalloc(c, &qoff, T + 1, "clique offsets")))
 			break;
-		const uint32_t grid = grid_for(c, T, SUP_THREADS / 32, 32);
-		k_clique_own<<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, T, inc.off, inc.third, inc.tri, own);
-		c.launches++;
+		const uint32_t grid = grid_for(c, (T + 31) / 32, SUP_THREADS / 32, 32);
 		if ((rc = scan_u32(c, own, qoff, T)))
 			break;
 		uint64_t Q = 0;
@@ -249,8 +310,6 @@ int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, CliqueCsr
 			break;
 		}
 		c.Q = Q;
-		c.release(own);
-		own = nullptr;
 		if (Q == 0)
 			break;
 		if ((rc = dalloc(c, &c.dquds, 4 * Q, "four-cliques")))

@@ -71,7 +71,7 @@ class Csr(C.Structure):
 
 class Opts(C.Structure):
     _fields_ = [("mem_budget_bytes", C.c_uint64), ("device", C.c_int),
-                ("parts", C.c_uint32), ("tune_table", C.c_char_p)]
+                ("parts", C.c_uint32), ("tune_table", C.c_char_p), ("flags", C.c_uint32)]
 
 
 class Result(C.Structure):
@@ -82,7 +82,8 @@ class Result(C.Structure):
                 ("t_support", C.c_double), ("t_cliques", C.c_double),
                 ("t_peel", C.c_double), ("t_total", C.c_double),
                 ("incidence_entries", C.c_uint64), ("gpu_launches", C.c_uint64),
-                ("peak_device_bytes", C.c_uint64), ("variant", C.c_int)]
+                ("peak_device_bytes", C.c_uint64), ("variant", C.c_int),
+                ("sum_te_sq", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -273,16 +274,19 @@ class Decomposition:
     extra: dict = field(default_factory=dict)
 
 
-def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1) -> Opts:
-    return Opts(mem_budget_bytes, device, parts, None)
+OPT_STAMP_PEEL = 0x1
+
+
+def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1, flags: int = 0) -> Opts:
+    return Opts(mem_budget_bytes, device, parts, None, flags)
 
 
 def decompose(g: HostGraph, variant="direct", device: int = 0, mem_budget_bytes: int = 0,
-              n_quds: int = 5, kfile: Optional[str] = None) -> Decomposition:
+              n_quds: int = 5, kfile: Optional[str] = None, flags: int = 0) -> Decomposition:
     """One-shot decomposition through nucleus34_decompose[_ondemand]."""
     L = lib()
     v = _VARIANTS[variant]
-    opts = make_opts(device, mem_budget_bytes)
+    opts = make_opts(device, mem_budget_bytes, flags=flags)
     res = Result()
     h = C.c_void_p()
     csr = g.csr()
@@ -310,9 +314,9 @@ def decompose(g: HostGraph, variant="direct", device: int = 0, mem_budget_bytes:
 class Context:
     """Device-resident context: upload once, run many times."""
 
-    def __init__(self, device: int = 0, mem_budget_bytes: int = 0):
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0, flags: int = 0):
         self._L = lib()
-        self._opts = make_opts(device, mem_budget_bytes)
+        self._opts = make_opts(device, mem_budget_bytes, flags=flags)
         self._h = C.c_void_p()
         _check(self._L.nucleus34_ctx_create(C.byref(self._opts), C.byref(self._h)), "ctx_create")
 

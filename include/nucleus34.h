@@ -71,7 +71,12 @@ typedef struct
 	int device;                /* CUDA ordinal */
 	uint32_t parts;            /* accepted for CLI parity (cuNucleus34.cu:161-169); one GPU */
 	const char *tune_table;    /* optional autotune table path, NULL = built-in defaults */
+	uint32_t flags;            /* NUCLEUS34_OPT_* bits, 0 = defaults */
 } nucleus34_opts;
+
+/* opts.flags: force the round-stamp ownership test in the on-demand peel
+ * (the default keeps death flags inside the incidence entries when T < 2^30). */
+#define NUCLEUS34_OPT_STAMP_PEEL 0x1u
 
 typedef struct
 {
@@ -92,6 +97,8 @@ typedef struct
 	uint64_t gpu_launches;        /* kernels this run launched */
 	uint64_t peak_device_bytes;   /* high-water mark of the library's device allocations */
 	int variant;                  /* NUCLEUS34_DIRECT or NUCLEUS34_ONDEMAND */
+	uint64_t sum_te_sq;           /* sum over edges of T(e)^2, T(e) = triangles on edge e
+	                                 (work measure of the 3-way intersections) */
 } nucleus34_result;
 
 typedef struct nucleus34_state *nucleus34_handle;

@@ -98,3 +98,17 @@ def test_budget_exceeded_is_reported(n34):
     with pytest.raises(n34.Nucleus34Error) as ei:
         n34.decompose(g, variant="direct", mem_budget_bytes=1 << 20)
     assert ei.value.code == n34.E_OOM_BUDGET
+
+
+@pytest.mark.parametrize("case", [("rmat", 12, 16, 1), ("rgg", 20000, 40, 8)])
+def test_stamp_peel_path_matches(n34, oracle, case):
+    """The round-stamp ownership test (used when T >= 2^30) gives the same k."""
+    if case[0] == "rmat":
+        s, t = n34.gen_rmat(case[1], case[2], case[3])
+    else:
+        s, t = n34.gen_rgg(case[1], case[2], case[3])
+    g = n34.graph_from_edges(s, t)
+    d = n34.decompose(g, variant="ondemand", flags=n34.OPT_STAMP_PEEL)
+    o = oracle.decompose(g)
+    assert np.array_equal(d.k, o.k)
+    assert d.result["four_clique_count"] == o.Q
