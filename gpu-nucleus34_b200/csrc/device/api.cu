@@ -233,6 +233,14 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 		N34_CUDA(cudaEventRecord(ev.e[1], c.stream));
 		r.triangle_count = c.T;
 		r.incidence_entries = 3 * c.T;
+		// The incidence is addressed with 32-bit positions, the limit the
+		// reference also enforces (cuNucleus34_ondemand.cu:505-511).
+		if (3 * c.T > 0xffffffffull)
+		{
+			rc = fail(NUCLEUS34_E_RANGE32, "incidence size " + std::to_string(3 * c.T) +
+											   " exceeds the 32-bit position range");
+			break;
+		}
 		if (c.T)
 		{
 			if ((rc = build_incidence(c, inc)))

@@ -16,6 +16,7 @@
 namespace n34 {
 
 int fail(int code, const std::string &msg);
+void clear_error();
 
 constexpr int WARP = 32;
 constexpr uint32_t FULL = 0xffffffffu;
@@ -34,6 +35,22 @@ __device__ __forceinline__ uint64_t lower_bound_u32(const uint32_t *__restrict__
 			lo = mid + 1;
 		else
 			hi = mid;
+	}
+	return lo;
+}
+
+// Same on 32-bit positions, branch-free: the trip count depends only on the
+// window length, so lanes searching the same window stay converged.
+__device__ __forceinline__ uint32_t lower_bound32(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi, uint32_t x)
+{
+	uint32_t n = hi - lo;
+	while (n > 0)
+	{
+		const uint32_t half = n >> 1;
+		const uint32_t mid = lo + half;
+		const bool less = __ldg(a + mid) < x;
+		lo = less ? mid + 1 : lo;
+		n = less ? n - half - 1 : half;
 	}
 	return lo;
 }

@@ -246,8 +246,9 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_ondemand(
 		const uint32_t t = F[i];
 		const uint32_t a = __ldg(tris + 3 * uint64_t(t)), b = __ldg(tris + 3 * uint64_t(t) + 1),
 					   c = __ldg(tris + 3 * uint64_t(t) + 2);
-		warp_intersect3(third, incO[a], incO[a + 1], incO[b], incO[b + 1], incO[c], incO[c + 1],
-						[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+		warp_intersect3(third, uint32_t(incO[a]), uint32_t(incO[a + 1]), uint32_t(incO[b]), uint32_t(incO[b + 1]),
+						uint32_t(incO[c]), uint32_t(incO[c + 1]),
+						[&](bool found, uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
 							uint32_t q0 = 0, q1 = 0, q2 = 0;
 							if (found)
 							{
@@ -367,9 +368,9 @@ __device__ __forceinline__ void entry_positions(uint32_t t, const uint32_t *__re
 	const uint32_t a = __ldg(tris + 3 * uint64_t(t)), b = __ldg(tris + 3 * uint64_t(t) + 1),
 				   c = __ldg(tris + 3 * uint64_t(t) + 2);
 	const uint32_t u = __ldg(src + b), v = __ldg(E + b), w = __ldg(E + c);
-	pos[0] = lower_bound_u32(third, incO[b], incO[b + 1], w);
-	pos[1] = lower_bound_u32(third, incO[a], incO[a + 1], v);
-	pos[2] = lower_bound_u32(third, incO[c], incO[c + 1], u);
+	pos[0] = lower_bound32(third, uint32_t(incO[b]), uint32_t(incO[b + 1]), w);
+	pos[1] = lower_bound32(third, uint32_t(incO[a]), uint32_t(incO[a + 1]), v);
+	pos[2] = lower_bound32(third, uint32_t(incO[c]), uint32_t(incO[c + 1]), u);
 }
 
 __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
@@ -438,10 +439,80 @@ __device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q
 		hit[2] = atomicSub(S + q2, 1) == level + 1;
 }
 
-// Debit of the dying triangles, hybrid like k_support: each warp takes 32
-// frontier entries; short drivers are intersected by their own lane, long ones
-// by the whole warp. Dead driver entries skip their searches.
-__global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags(
+__device__ __forceinline__ Driver frontier_driver(uint32_t t, const uint32_t *__restrict__ tris,
+												 const uint64_t *__restrict__ incO)
+{
+	const uint32_t ea = __ldg(tris + 3 * uint64_t(t)), eb = __ldg(tris + 3 * uint64_t(t) + 1),
+				   ec = __ldg(tris + 3 * uint64_t(t) + 2);
+	return pick_driver(uint32_t(incO[ea]), uint32_t(incO[ea + 1]), uint32_t(incO[eb]), uint32_t(incO[eb + 1]),
+					   uint32_t(incO[ec]), uint32_t(incO[ec + 1]));
+}
+
+// Debit of dying triangles whose shortest list is short: one thread each, so a
+// small frontier still spreads over the whole GPU.
+__global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
+	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
+	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
+	int32_t *__restrict__ S, uint64_t T)
+{
+	if (ctl->c.done)
+		return;
+	const uint32_t nF = ctl->c.nF;
+	const uint32_t *F = ctl->c.cur ? F1 : F0;
+	uint32_t *Fn = ctl->c.cur ? F0 : F1;
+	const int32_t level = int32_t(ctl->c.level);
+	uint32_t *nNext = &ctl->c.nNext;
+	uint32_t *err = &ctl->c.error;
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t fi = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; fi < nF; fi += stride)
+	{
+		const uint32_t t = F[fi];
+		const Driver d = frontier_driver(t, tris, incO);
+		if (d.ed - d.bd > THREAD_MODE_MAX)
+			continue; // the warp kernel takes it
+		uint32_t lo1 = d.lo1, lo2 = d.lo2;
+		for (uint32_t i = d.bd; i < d.ed && lo1 < d.hi1 && lo2 < d.hi2; ++i)
+		{
+			const uint32_t q0 = itri[i];
+			if (q0 & DEAD)
+				continue;
+			const uint32_t x = __ldg(third + i);
+			lo1 = lower_bound32(third, lo1, d.hi1, x);
+			if (lo1 >= d.hi1)
+				break;
+			if (__ldg(third + lo1) != x)
+				continue;
+			const uint32_t q1 = itri[lo1];
+			if (q1 & DEAD)
+				continue;
+			lo2 = lower_bound32(third, lo2, d.hi2, x);
+			if (lo2 >= d.hi2)
+				break;
+			if (__ldg(third + lo2) != x)
+				continue;
+			const uint32_t q2 = itri[lo2];
+			if (q2 & DEAD)
+				continue;
+			bool hit[3];
+			settle_flags(t, q0, q1, q2, S, level, hit);
+			const uint32_t qs[3] = {q0, q1, q2};
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+				if (hit[r])
+				{
+					const uint32_t slot = atomicAdd(nNext, 1u);
+					if (slot < T)
+						Fn[slot] = qs[r];
+					else
+						atomicOr(err, 1u);
+				}
+		}
+	}
+}
+
+// Debit of dying triangles with long lists: one warp each; lanes take 32
+// driver entries per step and binary-search the two other lists.
+__global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
 	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 	int32_t *__restrict__ S, uint64_t T)
@@ -457,124 +528,68 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags(
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
 	const uint32_t lane = lane_id();
-	for (uint64_t base = warp * 32; base < nF; base += nwarps * 32)
+	for (uint64_t fi = warp; fi < nF; fi += nwarps)
 	{
-		const uint64_t fi = base + lane;
-		const bool valid = fi < nF;
-		uint32_t t = 0;
-		Driver d{};
-		if (valid)
+		const uint32_t t = F[fi];
+		const Driver d = frontier_driver(t, tris, incO);
+		if (d.ed - d.bd <= THREAD_MODE_MAX)
+			continue; // the thread kernel took it (warp-uniform)
+		uint32_t lo1 = d.lo1, lo2 = d.lo2;
+		const uint32_t hi1 = d.hi1, hi2 = d.hi2;
+		for (uint32_t cb = d.bd; cb < d.ed; cb += 32)
 		{
-			t = F[fi];
-			const uint32_t ea = __ldg(tris + 3 * uint64_t(t)), eb = __ldg(tris + 3 * uint64_t(t) + 1),
-						   ec = __ldg(tris + 3 * uint64_t(t) + 2);
-			d = pick_driver(incO[ea], incO[ea + 1], incO[eb], incO[eb + 1], incO[ec], incO[ec + 1]);
-		}
-		const bool small = valid && d.ed - d.bd <= THREAD_MODE_MAX;
-		if (small)
-		{
-			uint64_t lo1 = d.lo1, lo2 = d.lo2;
-			for (uint64_t i = d.bd; i < d.ed && lo1 < d.hi1 && lo2 < d.hi2; ++i)
+			if (lo1 >= hi1 || lo2 >= hi2)
+				break; // warp-uniform
+			const uint32_t i = cb + lane;
+			const bool iv = i < d.ed;
+			uint32_t x = 0xffffffffu, q0 = DEAD, q1 = 0, q2 = 0;
+			if (iv)
 			{
-				const uint32_t q0 = itri[i];
-				if (q0 & DEAD)
-					continue;
-				const uint32_t x = __ldg(third + i);
-				lo1 = lower_bound_u32(third, lo1, d.hi1, x);
-				if (lo1 >= d.hi1)
-					break;
-				if (__ldg(third + lo1) != x)
-					continue;
-				const uint32_t q1 = itri[lo1];
-				if (q1 & DEAD)
-					continue;
-				lo2 = lower_bound_u32(third, lo2, d.hi2, x);
-				if (lo2 >= d.hi2)
-					break;
-				if (__ldg(third + lo2) != x)
-					continue;
-				const uint32_t q2 = itri[lo2];
-				if (q2 & DEAD)
-					continue;
-				bool hit[3];
-				settle_flags(t, q0, q1, q2, S, level, hit);
-				const uint32_t qs[3] = {q0, q1, q2};
-#pragma unroll
-				for (int r = 0; r < 3; ++r)
-					if (hit[r])
-					{
-						const uint32_t slot = atomicAdd(nNext, 1u);
-						if (slot < T)
-							Fn[slot] = qs[r];
-						else
-							atomicOr(err, 1u);
-					}
+				x = __ldg(third + i);
+				q0 = itri[i];
 			}
-		}
-		uint32_t large = __ballot_sync(FULL, valid && !small);
-		while (large)
-		{
-			const int j = __ffs(large) - 1;
-			large &= large - 1;
-			const uint32_t tj = __shfl_sync(FULL, t, j);
-			const uint64_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
-			uint64_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
-			uint64_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
-			for (uint64_t cb = bd; cb < ed; cb += 32)
+			uint32_t p1 = hi1, p2 = hi2;
+			bool s2 = false, found = false;
+			const bool s1 = iv && !(q0 & DEAD);
+			if (s1)
 			{
-				if (lo1 >= hi1 || lo2 >= hi2)
-					break; // warp-uniform
-				const uint64_t i = cb + lane;
-				const bool iv = i < ed;
-				uint32_t x = 0xffffffffu, q0 = DEAD, q1 = 0, q2 = 0;
-				if (iv)
+				p1 = lower_bound32(third, lo1, hi1, x);
+				if (p1 < hi1 && __ldg(third + p1) == x)
 				{
-					x = __ldg(third + i);
-					q0 = itri[i];
-				}
-				uint64_t p1 = hi1, p2 = hi2;
-				bool s2 = false, found = false;
-				const bool s1 = iv && !(q0 & DEAD);
-				if (s1)
-				{
-					p1 = lower_bound_u32(third, lo1, hi1, x);
-					if (p1 < hi1 && __ldg(third + p1) == x)
+					q1 = itri[p1];
+					if (!(q1 & DEAD))
 					{
-						q1 = itri[p1];
-						if (!(q1 & DEAD))
+						s2 = true;
+						p2 = lower_bound32(third, lo2, hi2, x);
+						if (p2 < hi2 && __ldg(third + p2) == x)
 						{
-							s2 = true;
-							p2 = lower_bound_u32(third, lo2, hi2, x);
-							if (p2 < hi2 && __ldg(third + p2) == x)
-							{
-								q2 = itri[p2];
-								found = !(q2 & DEAD);
-							}
+							q2 = itri[p2];
+							found = !(q2 & DEAD);
 						}
 					}
 				}
-				// later chunks hold larger x: the highest searching lane's
-				// lower bound stays valid for each list
-				const uint32_t m1 = __ballot_sync(FULL, s1), m2 = __ballot_sync(FULL, s2);
-				if (m1)
-					lo1 = __shfl_sync(FULL, p1, 31 - __clz(m1));
-				if (m2)
-					lo2 = __shfl_sync(FULL, p2, 31 - __clz(m2));
-				bool hit[3] = {false, false, false};
-				if (found)
-					settle_flags(tj, q0, q1, q2, S, level, hit);
-				const uint32_t qs[3] = {q0, q1, q2};
+			}
+			// later chunks hold larger x: the highest searching lane's lower
+			// bound stays valid for each list
+			const uint32_t m1 = __ballot_sync(FULL, s1), m2 = __ballot_sync(FULL, s2);
+			if (m1)
+				lo1 = __shfl_sync(FULL, p1, 31 - __clz(m1));
+			if (m2)
+				lo2 = __shfl_sync(FULL, p2, 31 - __clz(m2));
+			bool hit[3] = {false, false, false};
+			if (found)
+				settle_flags(t, q0, q1, q2, S, level, hit);
+			const uint32_t qs[3] = {q0, q1, q2};
 #pragma unroll
-				for (int r = 0; r < 3; ++r)
+			for (int r = 0; r < 3; ++r)
+			{
+				const uint32_t slot = warp_append(hit[r], nNext);
+				if (hit[r])
 				{
-					const uint32_t slot = warp_append(hit[r], nNext);
-					if (hit[r])
-					{
-						if (slot < T)
-							Fn[slot] = qs[r];
-						else
-							atomicOr(err, 1u);
-					}
+					if (slot < T)
+						Fn[slot] = qs[r];
+					else
+						atomicOr(err, 1u);
 				}
 			}
 		}
@@ -686,8 +701,10 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			{
 				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.off,
 																   inc.third, inc.tri, 3 * T);
-				k_debit_flags<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off, inc.third,
-																	inc.tri, S, T);
+				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off,
+																		   inc.third, inc.tri, S, T);
+				k_debit_flags_warp<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off, inc.third,
+																		 inc.tri, S, T);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, c.dsrc, c.dE, inc.off,
 																	   inc.third, inc.tri, 3 * T);
 			}
@@ -704,7 +721,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			}
 			k_advance<<<1, 1, 0, c.stream>>>(ctl);
 		};
-		const uint32_t per_round = flags ? 7u : 6u;
+		const uint32_t per_round = flags ? 8u : 6u;
 		// Rounds are replayed from a CUDA graph of ROUNDS_PER_GRAPH rounds; the
 		// host reads one flag per replay. Rounds after the last one are no-ops.
 		constexpr uint32_t ROUNDS_PER_GRAPH = 16;

@@ -25,7 +25,7 @@ constexpr int SUP_THREADS = 256;
 
 struct TriEdges
 {
-	uint64_t b0, e0, b1, e1, b2, e2;
+	uint32_t b0, e0, b1, e1, b2, e2;
 };
 
 __device__ __forceinline__ TriEdges tri_lists(const uint32_t *__restrict__ tris, const uint64_t *__restrict__ incO,
@@ -33,12 +33,12 @@ __device__ __forceinline__ TriEdges tri_lists(const uint32_t *__restrict__ tris,
 {
 	const uint32_t a = __ldg(tris + 3 * t + 0), b = __ldg(tris + 3 * t + 1), c = __ldg(tris + 3 * t + 2);
 	TriEdges L;
-	L.b0 = incO[a];
-	L.e0 = incO[a + 1];
-	L.b1 = incO[b];
-	L.e1 = incO[b + 1];
-	L.b2 = incO[c];
-	L.e2 = incO[c + 1];
+	L.b0 = uint32_t(incO[a]);
+	L.e0 = uint32_t(incO[a + 1]);
+	L.b1 = uint32_t(incO[b]);
+	L.e1 = uint32_t(incO[b + 1]);
+	L.b2 = uint32_t(incO[c]);
+	L.e2 = uint32_t(incO[c + 1]);
 	return L;
 }
 
@@ -48,7 +48,7 @@ __device__ __forceinline__ TriEdges tri_lists(const uint32_t *__restrict__ tris,
 // counts the cliques whose lowest triangle id is t (the direct variant's
 // clique-list sizes), from the partner ids the intersection located.
 template <bool WITH_OWN>
-__global__ void __launch_bounds__(SUP_THREADS) k_support(const uint32_t *__restrict__ tris, uint64_t T,
+__global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__restrict__ tris, uint64_t T,
 														 const uint64_t *__restrict__ incO,
 														 const uint32_t *__restrict__ third,
 														 const uint32_t *__restrict__ itri,
@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(SUP_THREADS) k_support(const uint32_t *__restr
 		if (small)
 		{
 			uint32_t cnt = 0, mine = 0;
-			thread_intersect3(third, d, [&](uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+			thread_intersect3(third, d, [&](uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
 				++cnt;
 				if (WITH_OWN)
 					mine += uint32_t(t) < __ldg(itri + pd) && uint32_t(t) < __ldg(itri + p1) &&
@@ -90,12 +90,12 @@ __global__ void __launch_bounds__(SUP_THREADS) k_support(const uint32_t *__restr
 			const int j = __ffs(large) - 1;
 			large &= large - 1;
 			const uint64_t tj = base + uint64_t(j);
-			const uint64_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
-			const uint64_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
-			const uint64_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
+			const uint32_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
+			const uint32_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
+			const uint32_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
 			uint32_t cnt = 0, mine = 0;
 			warp_intersect3(third, bd, ed, lo1, hi1, lo2, hi2,
-							[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+							[&](bool found, uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
 								cnt += __popc(__ballot_sync(FULL, found));
 								if (WITH_OWN)
 								{
@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__
 		const bool small = work && d.ed - d.bd <= THREAD_MODE_MAX;
 		if (small)
 		{
-			thread_intersect3(third, d, [&](uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+			thread_intersect3(third, d, [&](uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
 				uint32_t q0 = __ldg(itri + pd), q1 = __ldg(itri + p1), q2 = __ldg(itri + p2);
 				if (uint32_t(t) < q0 && uint32_t(t) < q1 && uint32_t(t) < q2 && out < out_end)
 				{
@@ -193,11 +193,11 @@ __global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__
 			const uint32_t tj = uint32_t(base) + uint32_t(j);
 			uint64_t o = __shfl_sync(FULL, out, j);
 			const uint64_t oe = __shfl_sync(FULL, out_end, j);
-			const uint64_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
-			const uint64_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
-			const uint64_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
+			const uint32_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
+			const uint32_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
+			const uint32_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
 			warp_intersect3(third, bd, ed, lo1, hi1, lo2, hi2,
-							[&](bool found, uint32_t, uint64_t pd, uint64_t p1, uint64_t p2) {
+							[&](bool found, uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
 								bool mine = false;
 								uint32_t q0 = 0, q1 = 0, q2 = 0;
 								if (found)
