@@ -22,6 +22,11 @@ struct CliqueCsr
 };
 
 int build_src(Ctx &c);
+// Triangle-listing passes on caller-owned memory (no bitmap cache).
+cudaError_t launch_tri_count(const uint32_t *O, const uint32_t *E, uint64_t n, uint32_t *cnt, int sm_count,
+							 cudaStream_t s);
+cudaError_t launch_tri_write(const uint32_t *O, const uint32_t *E, uint64_t n, const uint64_t *toff,
+							 uint32_t *tris, int sm_count, cudaStream_t s);
 int list_triangles(Ctx &c);
 int build_incidence(Ctx &c, Incidence &inc);
 void free_incidence(Ctx &c, Incidence &inc);

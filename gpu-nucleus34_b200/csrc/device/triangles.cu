@@ -168,6 +168,26 @@ int build_src(Ctx &c)
 	return NUCLEUS34_OK;
 }
 
+// Launch helpers for callers that manage their own memory (no context):
+// pass 1 (counts only, no bitmap) and pass 2 (recomputing the membership tests).
+cudaError_t launch_tri_count(const uint32_t *O, const uint32_t *E, uint64_t n, uint32_t *cnt, int sm_count,
+							 cudaStream_t s)
+{
+	uint64_t g = (n + TRI_WARPS - 1) / TRI_WARPS;
+	g = g > uint64_t(sm_count) * 32 ? uint64_t(sm_count) * 32 : (g ? g : 1);
+	k_tri_count<<<uint32_t(g), TRI_THREADS, 0, s>>>(O, E, n, nullptr, nullptr, cnt);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_tri_write(const uint32_t *O, const uint32_t *E, uint64_t n, const uint64_t *toff,
+							 uint32_t *tris, int sm_count, cudaStream_t s)
+{
+	uint64_t g = (n + TRI_WARPS - 1) / TRI_WARPS;
+	g = g > uint64_t(sm_count) * 32 ? uint64_t(sm_count) * 32 : (g ? g : 1);
+	k_tri_write<<<uint32_t(g), TRI_THREADS, 0, s>>>(O, E, n, nullptr, nullptr, toff, tris);
+	return cudaGetLastError();
+}
+
 // Lists the triangles of the resident graph into c.dtris (3*T u32) and sets c.T.
 int list_triangles(Ctx &c)
 {

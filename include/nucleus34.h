@@ -149,6 +149,29 @@ int nucleus34_ctx_run(nucleus34_ctx ctx, int variant, nucleus34_result *res);
 int nucleus34_ctx_copy_k(nucleus34_ctx ctx, int32_t *k_out, uint32_t *tris_out);
 void nucleus34_ctx_destroy(nucleus34_ctx ctx);
 
+/* ---- triangle listing without allocation --------------------------------- */
+
+/* No counterpart in the reference. For callers that cannot allocate device
+ * memory while they run (all of HBM reserved up front by their own pool, a
+ * framework allocator that must not be bypassed, latency-critical loops):
+ * lists the triangles of an oriented CSR already in device memory, in
+ * canonical (a,b) order, into a caller-owned device buffer, and allocates
+ * nothing. d_O holds n+1 offsets (O[n] = m), d_E the m destinations; d_tris
+ * receives 3 u32 per triangle. The count is always returned in
+ * *triangle_count; if it exceeds tris_capacity nothing is written and the
+ * call returns NUCLEUS34_E_INVALID (call again with room; capacity 0 and a
+ * NULL d_tris is a count-only query). At most 2^20 vertices: larger graphs
+ * are rejected with NUCLEUS34_E_INVALID. The temporaries live in a fixed
+ * static device array (about 12.6 MB, held by every GPU that loads the
+ * library until exit) shared by all calls: calls that overlap on one GPU race
+ * and must be serialised by the caller. The first call on a device resolves
+ * that array's address on that device; make that first call before any stream
+ * capture. stream is a cudaStream_t (NULL = default stream); the call
+ * synchronises it before returning. */
+int nucleus34_list_triangles_noalloc(const uint32_t *d_O, const uint32_t *d_E, uint64_t n, uint64_t m,
+									 uint32_t *d_tris, uint64_t tris_capacity, uint64_t *triangle_count,
+									 int device, void *stream);
+
 /* ---- host graph layer (reference reader/orientation semantics) ----------- */
 
 /* Library-owned oriented CSR; O has n+1 entries here. */
