@@ -221,6 +221,62 @@ __global__ void k_inc_split(const unsigned long long *__restrict__ keys, uint64_
 	}
 }
 
+// Live entries per edge (warp per edge, coalesced reads of the tri column).
+__global__ void k_alive_count(const uint64_t *__restrict__ off, uint64_t m, const uint32_t *__restrict__ tri,
+							  uint32_t *__restrict__ cnt)
+{
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	const uint32_t lane = lane_id();
+	for (uint64_t e = warp; e < m; e += nwarps)
+	{
+		const uint64_t b = off[e], en = off[e + 1];
+		uint32_t live = 0;
+		for (uint64_t i = b + lane; i < en; i += 32)
+			live += !(tri[i] & INC_DEAD);
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1)
+			live += __shfl_xor_sync(FULL, live, o);
+		if (lane == 0)
+			cnt[e] = live;
+	}
+}
+
+// Stable per-edge copy of the live entries into their new segment (order by
+// third vertex is kept, so every list stays sorted).
+__global__ void k_compact_copy(const uint64_t *__restrict__ off, const uint64_t *__restrict__ noff, uint64_t m,
+							   const uint32_t *__restrict__ third, const uint32_t *__restrict__ tri,
+							   uint32_t *__restrict__ third2, uint32_t *__restrict__ tri2)
+{
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	const uint32_t lane = lane_id();
+	for (uint64_t e = warp; e < m; e += nwarps)
+	{
+		const uint64_t b = off[e], en = off[e + 1];
+		uint64_t out = noff[e];
+		for (uint64_t base = b; base < en; base += 32)
+		{
+			const uint64_t i = base + lane;
+			uint32_t t = INC_DEAD, x = 0;
+			if (i < en)
+			{
+				t = tri[i];
+				x = third[i];
+			}
+			const bool keep = !(t & INC_DEAD);
+			const uint32_t bal = __ballot_sync(FULL, keep);
+			if (keep)
+			{
+				const uint64_t o = out + __popc(bal & ((1u << lane) - 1u));
+				third2[o] = x;
+				tri2[o] = t;
+			}
+			out += __popc(bal);
+		}
+	}
+}
+
 } // namespace
 
 int build_incidence(Ctx &c, Incidence &inc)
@@ -344,6 +400,62 @@ int build_incidence(Ctx &c, Incidence &inc)
 			rc = fail(NUCLEUS34_E_CUDA, "incidence kernels");
 	} while (false);
 	cleanup();
+	return rc;
+}
+
+int compact_incidence(Ctx &c, Incidence &inc, uint64_t *kept)
+{
+	const uint64_t m = c.m, n3 = 3 * c.T;
+	uint32_t *cnt = nullptr, *third2 = nullptr, *tri2 = nullptr;
+	uint64_t *noff = nullptr;
+	int rc = NUCLEUS34_OK;
+	do
+	{
+		if ((rc = dalloc(c, &cnt, m ? m : 1, "compaction counts")))
+			break;
+		if ((rc = dalloc(c, &noff, m + 1, "compaction offsets")))
+			break;
+		const uint32_t gw = grid_for(c, m, 256 / 32, 16);
+		k_alive_count<<<gw, 256, 0, c.stream>>>(inc.off, m, inc.tri, cnt);
+		c.launches++;
+		if ((rc = scan_u32(c, cnt, noff, m)))
+			break;
+		uint64_t live = 0;
+		if (cudaMemcpyAsync(&live, noff + m, 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "compaction count");
+			break;
+		}
+		if (live > n3)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "internal: compaction count");
+			break;
+		}
+		const uint64_t cap = live ? live : 1;
+		if ((rc = dalloc(c, &third2, cap, "compaction third")))
+			break;
+		if ((rc = dalloc(c, &tri2, cap, "compaction tri")))
+			break;
+		k_compact_copy<<<gw, 256, 0, c.stream>>>(inc.off, noff, m, inc.third, inc.tri, third2, tri2);
+		c.launches++;
+		// Copy back into the same arrays so that kernels captured with these
+		// pointers stay valid.
+		if ((live && (cudaMemcpyAsync(inc.third, third2, live * 4, cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess ||
+					  cudaMemcpyAsync(inc.tri, tri2, live * 4, cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess)) ||
+			cudaMemcpyAsync(inc.off, noff, (m + 1) * 8, cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess ||
+			cudaGetLastError() != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "compaction copy");
+			break;
+		}
+		if (kept)
+			*kept = live;
+	} while (false);
+	c.release(cnt);
+	c.release(noff);
+	c.release(third2);
+	c.release(tri2);
 	return rc;
 }
 

@@ -1,124 +1,149 @@
-// Warp-cooperative 3-way intersection of a triangle's three incidence lists.
+// Intersection of a triangle's incidence lists.
 //
 // Reference: for_each_clique_of (nucleus/cuNucleus34_ondemand.cu:136-170) walks
-// the three lists with one thread in a 3-way zipper, O(|L(a)|+|L(b)|+|L(c)|)
-// dependent steps per triangle. Here the shortest list drives: each lane takes
-// one entry x of it and binary-searches x in the other two lists; a ballot
-// over the 32 lanes yields the common thirds of 32 driver entries per step.
-// After each step the search windows of the other lists start at the position
-// lane 31 reached (the driver is sorted, so later x are larger).
+// the three lists of triangle t=(u,v,w) in one thread with a 3-way zipper,
+// O(|L(a)|+|L(b)|+|L(c)|) dependent steps.
+//
+// Two facts shape the device version:
+//  1. Any two of the three lists suffice to find the cliques: x in L(u,w) and
+//     in L(u,v) is adjacent to u, v and w, so {u,v,w,x} is a four-clique and x
+//     is in L(v,w) as well. The common thirds of the two SHORTEST lists are
+//     exactly t's cliques; the longest list is only searched, for a found x,
+//     when the partner triangle on that edge is needed.
+//  2. On skewed graphs the two shortest lists are usually of similar length,
+//     so a merge beats per-entry binary searches. One warp merges 32 + 32
+//     entries per step with coalesced loads: each lane locates its A entry in
+//     the B tile held in registers by a 5-step shuffle search, and the tile
+//     whose last entry is smaller is consumed. When B is far longer than A,
+//     the lanes binary-search B instead; short A lists are handled by a single
+//     lane (see THREAD_MODE_MAX).
 #pragma once
 
 #include "common.cuh"
 
 namespace n34 {
 
-// f(found, x, pd, p1, p2) is called by ALL lanes once per 32-entry step (so it
-// may use warp collectives); pd/p1/p2 are positions in third[]/tri[] of x in
-// the driver list and the two other lists (valid only when found). Positions
-// are 32-bit: the incidence holds 3T < 2^32 entries (checked by the driver).
-template <class F>
-__device__ __forceinline__ void warp_intersect3(const uint32_t *__restrict__ third, uint32_t b0, uint32_t e0,
-												uint32_t b1, uint32_t e1, uint32_t b2, uint32_t e2, F &&f)
+// A triangle's three lists as [begin, end) positions in third[] / tri[],
+// ordered by length: A shortest, B middle, C longest. Positions are 32-bit:
+// the incidence holds 3T < 2^32 entries (checked before it is built).
+struct Lists
 {
-	// pick the shortest list as the driver
-	uint32_t bd = b0, ed = e0, lo1 = b1, hi1 = e1, lo2 = b2, hi2 = e2;
-	if (e1 - b1 < ed - bd)
-	{
-		bd = b1;
-		ed = e1;
-		lo1 = b0;
-		hi1 = e0;
-	}
-	if (e2 - b2 < ed - bd)
-	{
-		// driver becomes list 2; the previous driver moves into slot 2
-		lo2 = bd;
-		hi2 = ed;
-		bd = b2;
-		ed = e2;
-	}
-	const uint32_t lane = lane_id();
-	for (uint32_t base = bd; base < ed; base += 32)
-	{
-		if (lo1 >= hi1 || lo2 >= hi2)
-			break; // warp-uniform
-		const uint32_t i = base + lane;
-		const bool valid = i < ed;
-		const uint32_t x = valid ? __ldg(third + i) : 0xffffffffu;
-		uint32_t p1 = hi1, p2 = hi2;
-		bool found = false;
-		if (valid)
-		{
-			p1 = lower_bound32(third, lo1, hi1, x);
-			if (p1 < hi1 && __ldg(third + p1) == x)
-			{
-				p2 = lower_bound32(third, lo2, hi2, x);
-				found = p2 < hi2 && __ldg(third + p2) == x;
-			}
-		}
-		f(found, x, i, p1, p2);
-		// later chunks hold larger x: the highest lane that searched a list
-		// leaves a lower bound that stays valid for that list
-		const uint32_t m1 = __ballot_sync(FULL, valid);
-		const uint32_t m2 = __ballot_sync(FULL, valid && p1 < hi1 && __ldg(third + p1) == x);
-		if (m1)
-			lo1 = __shfl_sync(FULL, p1, 31 - __clz(m1));
-		if (m2)
-			lo2 = __shfl_sync(FULL, p2, 31 - __clz(m2));
-	}
-}
-
-// The shortest of the three lists drives; the other two are searched.
-struct Driver
-{
-	uint32_t bd, ed, lo1, hi1, lo2, hi2;
+	uint32_t a0, a1, b0, b1, c0, c1;
 };
 
-__device__ __forceinline__ Driver pick_driver(uint32_t b0, uint32_t e0, uint32_t b1, uint32_t e1, uint32_t b2,
-											  uint32_t e2)
+__device__ __forceinline__ Lists order_lists(uint32_t x0, uint32_t x1, uint32_t y0, uint32_t y1, uint32_t z0,
+											 uint32_t z1)
 {
-	Driver d{b0, e0, b1, e1, b2, e2};
-	if (e1 - b1 < d.ed - d.bd)
+	// sort three (begin, end) pairs by length
+	uint32_t p0 = x0, p1 = x1, q0 = y0, q1 = y1, r0 = z0, r1 = z1, t;
+	if (q1 - q0 < p1 - p0)
 	{
-		d.bd = b1;
-		d.ed = e1;
-		d.lo1 = b0;
-		d.hi1 = e0;
+		t = p0; p0 = q0; q0 = t;
+		t = p1; p1 = q1; q1 = t;
 	}
-	if (e2 - b2 < d.ed - d.bd)
+	if (r1 - r0 < q1 - q0)
 	{
-		d.lo2 = d.bd;
-		d.hi2 = d.ed;
-		d.bd = b2;
-		d.ed = e2;
+		t = q0; q0 = r0; r0 = t;
+		t = q1; q1 = r1; r1 = t;
 	}
-	return d;
+	if (q1 - q0 < p1 - p0)
+	{
+		t = p0; p0 = q0; q0 = t;
+		t = p1; p1 = q1; q1 = t;
+	}
+	return Lists{p0, p1, q0, q1, r0, r1};
 }
 
-// Driver length up to which one lane handles a triangle on its own (the
-// lanes of a warp then work on 32 different triangles at once).
+// Shortest-list length up to which one lane handles a triangle on its own.
 constexpr uint32_t THREAD_MODE_MAX = 16;
+// B longer than this multiple of A: binary-search B instead of merging.
+constexpr uint32_t MERGE_RATIO = 24;
 
-// Thread-local 3-way intersection for a short driver list: f(x, pd, p1, p2)
-// per common third. Windows only move forward because the driver is sorted.
-template <class F>
-__device__ __forceinline__ void thread_intersect3(const uint32_t *__restrict__ third, Driver d, F &&f)
+__device__ __forceinline__ bool use_merge(const Lists &L)
 {
-	for (uint32_t i = d.bd; i < d.ed && d.lo1 < d.hi1 && d.lo2 < d.hi2; ++i)
+	return (L.b1 - L.b0) <= MERGE_RATIO * (L.a1 - L.a0);
+}
+
+// Warp tile merge of A and B. f(found, x, pa, pb) is called by all lanes once
+// per step; found lanes hold x = third[pa] = third[pb]. Each common x is seen
+// exactly once, in ascending order across steps.
+template <class F>
+__device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, uint32_t a0, uint32_t a1, uint32_t b0,
+											uint32_t b1, F &&f)
+{
+	const uint32_t lane = lane_id();
+	while (a0 < a1 && b0 < b1) // warp-uniform
+	{
+		const uint32_t ai = a0 + lane, bi = b0 + lane;
+		const bool av_ok = ai < a1, bv_ok = bi < b1;
+		const uint32_t av = av_ok ? __ldg(third + ai) : 0xffffffffu;
+		const uint32_t bv = bv_ok ? __ldg(third + bi) : 0xffffffffu;
+		const uint32_t amax = __shfl_sync(FULL, av, 31), bmax = __shfl_sync(FULL, bv, 31);
+		const uint32_t m = amax < bmax ? amax : bmax;
+		// first lane j of the B tile with bv_j >= av (31 if none: then no match)
+		uint32_t pos = 0;
+#pragma unroll
+		for (uint32_t step = 16; step > 0; step >>= 1)
+		{
+			const uint32_t probe = __shfl_sync(FULL, bv, (pos + step - 1) & 31);
+			if (probe < av)
+				pos += step;
+		}
+		const uint32_t hitv = __shfl_sync(FULL, bv, pos & 31);
+		const bool found = av_ok && av <= m && hitv == av && b0 + pos < b1;
+		f(found, av, ai, b0 + pos);
+		// everything <= m is consumed; at least one tile is used up entirely
+		a0 += __popc(__ballot_sync(FULL, av_ok && av <= m));
+		b0 += __popc(__ballot_sync(FULL, bv_ok && bv <= m));
+	}
+}
+
+// Warp binary search of A's entries in B (B much longer than A).
+template <class F>
+__device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third, uint32_t a0, uint32_t a1, uint32_t b0,
+											 uint32_t b1, F &&f)
+{
+	const uint32_t lane = lane_id();
+	for (uint32_t base = a0; base < a1; base += 32)
+	{
+		if (b0 >= b1)
+			break; // warp-uniform
+		const uint32_t ai = base + lane;
+		const bool ok = ai < a1;
+		const uint32_t x = ok ? __ldg(third + ai) : 0xffffffffu;
+		uint32_t p = b1;
+		if (ok)
+			p = lower_bound32(third, b0, b1, x);
+		const bool found = ok && p < b1 && __ldg(third + p) == x;
+		f(found, x, ai, p);
+		// later steps hold larger x: the highest searching lane's bound stays valid
+		const uint32_t msk = __ballot_sync(FULL, ok);
+		b0 = __shfl_sync(FULL, p, 31 - __clz(msk));
+	}
+}
+
+// Warp dispatch between merge and search for the two shortest lists.
+template <class F>
+__device__ __forceinline__ void warp_intersect2(const uint32_t *__restrict__ third, const Lists &L, F &&f)
+{
+	if (use_merge(L))
+		warp_merge2(third, L.a0, L.a1, L.b0, L.b1, f);
+	else
+		warp_search2(third, L.a0, L.a1, L.b0, L.b1, f);
+}
+
+// One lane on its own: each entry of A binary-searched in B (the window only
+// moves forward). f(x, pa, pb) per common x, ascending.
+template <class F>
+__device__ __forceinline__ void lane_intersect2(const uint32_t *__restrict__ third, const Lists &L, F &&f)
+{
+	uint32_t lo = L.b0;
+	for (uint32_t i = L.a0; i < L.a1 && lo < L.b1; ++i)
 	{
 		const uint32_t x = __ldg(third + i);
-		d.lo1 = lower_bound32(third, d.lo1, d.hi1, x);
-		if (d.lo1 >= d.hi1)
-			break;
-		if (__ldg(third + d.lo1) != x)
-			continue;
-		d.lo2 = lower_bound32(third, d.lo2, d.hi2, x);
-		if (d.lo2 >= d.hi2)
-			break;
-		if (__ldg(third + d.lo2) != x)
-			continue;
-		f(x, i, d.lo1, d.lo2);
+		lo = lower_bound32(third, lo, L.b1, x);
+		if (lo < L.b1 && __ldg(third + lo) == x)
+			f(x, i, lo);
 	}
 }
 

@@ -25,6 +25,9 @@
 //   advance            swap frontiers, advance the round.
 // The result is independent of thread timing: ownership depends only on the
 // stamps, and crossing detection catches every triangle that reaches the level.
+#include <cstdio>
+#include <vector>
+
 #include "intersect.cuh"
 #include "pipeline.cuh"
 
@@ -227,6 +230,18 @@ __device__ __forceinline__ void settle_clique(bool found, uint32_t t, uint32_t p
 	}
 }
 
+__device__ __forceinline__ Lists frontier_lists(uint32_t t, const uint32_t *__restrict__ tris,
+											   const uint64_t *__restrict__ incO)
+{
+	const uint32_t ea = __ldg(tris + 3 * uint64_t(t)), eb = __ldg(tris + 3 * uint64_t(t) + 1),
+				   ec = __ldg(tris + 3 * uint64_t(t) + 2);
+	return order_lists(uint32_t(incO[ea]), uint32_t(incO[ea + 1]), uint32_t(incO[eb]), uint32_t(incO[eb + 1]),
+					   uint32_t(incO[ec]), uint32_t(incO[ec + 1]));
+}
+
+// On-demand debit with the round-stamp owner test (used when triangle ids do
+// not leave room for flag bits): one warp per dying triangle; the partner on
+// the longest list is found by a forward-moving binary search.
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_ondemand(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
 	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
@@ -244,20 +259,23 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_ondemand(
 	for (uint64_t i = warp; i < nF; i += nwarps)
 	{
 		const uint32_t t = F[i];
-		const uint32_t a = __ldg(tris + 3 * uint64_t(t)), b = __ldg(tris + 3 * uint64_t(t) + 1),
-					   c = __ldg(tris + 3 * uint64_t(t) + 2);
-		warp_intersect3(third, uint32_t(incO[a]), uint32_t(incO[a + 1]), uint32_t(incO[b]), uint32_t(incO[b + 1]),
-						uint32_t(incO[c]), uint32_t(incO[c + 1]),
-						[&](bool found, uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
-							uint32_t q0 = 0, q1 = 0, q2 = 0;
-							if (found)
-							{
-								q0 = __ldg(itri + pd);
-								q1 = __ldg(itri + p1);
-								q2 = __ldg(itri + p2);
-							}
-							settle_clique(found, t, q0, q1, q2, K, R, S, round, level, Fn, &ctl->c.nNext, T, &ctl->c.error);
-						});
+		const Lists L = frontier_lists(t, tris, incO);
+		uint32_t lo_c = L.c0;
+		warp_intersect2(third, L, [&](bool found, uint32_t x, uint32_t pa, uint32_t pb) {
+			const uint32_t fm = __ballot_sync(FULL, found);
+			if (!fm)
+				return;
+			const uint32_t pc = found ? lower_bound32(third, lo_c, L.c1, x) : L.c1;
+			lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
+			uint32_t q0 = 0, q1 = 0, q2 = 0;
+			if (found)
+			{
+				q0 = __ldg(itri + pa);
+				q1 = __ldg(itri + pb);
+				q2 = __ldg(itri + pc);
+			}
+			settle_clique(found, t, q0, q1, q2, K, R, S, round, level, Fn, &ctl->c.nNext, T, &ctl->c.error);
+		});
 	}
 }
 
@@ -355,7 +373,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_direct(
 // entry's triangle id means "died in an earlier round", bit 30 "dies in this
 // round". The owner rule then reads nothing but the three entries the 3-way
 // intersection already located, and a dead driver entry skips its searches.
-constexpr uint32_t DEAD = 0x80000000u;
+constexpr uint32_t DEAD = INC_DEAD;
 constexpr uint32_t DYING = 0x40000000u;
 constexpr uint32_t ID_MASK = 0x3fffffffu;
 
@@ -439,17 +457,11 @@ __device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q
 		hit[2] = atomicSub(S + q2, 1) == level + 1;
 }
 
-__device__ __forceinline__ Driver frontier_driver(uint32_t t, const uint32_t *__restrict__ tris,
-												 const uint64_t *__restrict__ incO)
-{
-	const uint32_t ea = __ldg(tris + 3 * uint64_t(t)), eb = __ldg(tris + 3 * uint64_t(t) + 1),
-				   ec = __ldg(tris + 3 * uint64_t(t) + 2);
-	return pick_driver(uint32_t(incO[ea]), uint32_t(incO[ea + 1]), uint32_t(incO[eb]), uint32_t(incO[eb + 1]),
-					   uint32_t(incO[ec]), uint32_t(incO[ec + 1]));
-}
-
 // Debit of dying triangles whose shortest list is short: one thread each, so a
-// small frontier still spreads over the whole GPU.
+// small frontier still spreads over the whole GPU. Dead entries of the
+// shortest list are skipped before any search. After a compaction the entry
+// of a partner that died earlier is gone; a third that is not found on an edge
+// therefore means the clique was destroyed before.
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
 	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
@@ -467,30 +479,28 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	for (uint64_t fi = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; fi < nF; fi += stride)
 	{
 		const uint32_t t = F[fi];
-		const Driver d = frontier_driver(t, tris, incO);
-		if (d.ed - d.bd > THREAD_MODE_MAX)
+		const Lists L = frontier_lists(t, tris, incO);
+		if (L.a1 - L.a0 > THREAD_MODE_MAX)
 			continue; // the warp kernel takes it
-		uint32_t lo1 = d.lo1, lo2 = d.lo2;
-		for (uint32_t i = d.bd; i < d.ed && lo1 < d.hi1 && lo2 < d.hi2; ++i)
+		uint32_t lo_b = L.b0, lo_c = L.c0;
+		for (uint32_t i = L.a0; i < L.a1 && lo_b < L.b1; ++i)
 		{
 			const uint32_t q0 = itri[i];
 			if (q0 & DEAD)
 				continue;
 			const uint32_t x = __ldg(third + i);
-			lo1 = lower_bound32(third, lo1, d.hi1, x);
-			if (lo1 >= d.hi1)
+			lo_b = lower_bound32(third, lo_b, L.b1, x);
+			if (lo_b >= L.b1)
 				break;
-			if (__ldg(third + lo1) != x)
+			if (__ldg(third + lo_b) != x)
 				continue;
-			const uint32_t q1 = itri[lo1];
+			const uint32_t q1 = itri[lo_b];
 			if (q1 & DEAD)
 				continue;
-			lo2 = lower_bound32(third, lo2, d.hi2, x);
-			if (lo2 >= d.hi2)
-				break;
-			if (__ldg(third + lo2) != x)
-				continue;
-			const uint32_t q2 = itri[lo2];
+			lo_c = lower_bound32(third, lo_c, L.c1, x);
+			if (lo_c >= L.c1 || __ldg(third + lo_c) != x)
+				continue; // the partner on the longest list was compacted away
+			const uint32_t q2 = itri[lo_c];
 			if (q2 & DEAD)
 				continue;
 			bool hit[3];
@@ -510,8 +520,9 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	}
 }
 
-// Debit of dying triangles with long lists: one warp each; lanes take 32
-// driver entries per step and binary-search the two other lists.
+// Debit of dying triangles with long lists: one warp each, tile merge (or
+// binary search) of the two shortest lists; a found x is looked up in the
+// longest list only when its two other partners are still alive.
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
 	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
@@ -527,58 +538,35 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 	uint32_t *err = &ctl->c.error;
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-	const uint32_t lane = lane_id();
 	for (uint64_t fi = warp; fi < nF; fi += nwarps)
 	{
 		const uint32_t t = F[fi];
-		const Driver d = frontier_driver(t, tris, incO);
-		if (d.ed - d.bd <= THREAD_MODE_MAX)
+		const Lists L = frontier_lists(t, tris, incO);
+		if (L.a1 - L.a0 <= THREAD_MODE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
-		uint32_t lo1 = d.lo1, lo2 = d.lo2;
-		const uint32_t hi1 = d.hi1, hi2 = d.hi2;
-		for (uint32_t cb = d.bd; cb < d.ed; cb += 32)
-		{
-			if (lo1 >= hi1 || lo2 >= hi2)
-				break; // warp-uniform
-			const uint32_t i = cb + lane;
-			const bool iv = i < d.ed;
-			uint32_t x = 0xffffffffu, q0 = DEAD, q1 = 0, q2 = 0;
-			if (iv)
-			{
-				x = __ldg(third + i);
-				q0 = itri[i];
-			}
-			uint32_t p1 = hi1, p2 = hi2;
-			bool s2 = false, found = false;
-			const bool s1 = iv && !(q0 & DEAD);
-			if (s1)
-			{
-				p1 = lower_bound32(third, lo1, hi1, x);
-				if (p1 < hi1 && __ldg(third + p1) == x)
-				{
-					q1 = itri[p1];
-					if (!(q1 & DEAD))
-					{
-						s2 = true;
-						p2 = lower_bound32(third, lo2, hi2, x);
-						if (p2 < hi2 && __ldg(third + p2) == x)
-						{
-							q2 = itri[p2];
-							found = !(q2 & DEAD);
-						}
-					}
-				}
-			}
-			// later chunks hold larger x: the highest searching lane's lower
-			// bound stays valid for each list
-			const uint32_t m1 = __ballot_sync(FULL, s1), m2 = __ballot_sync(FULL, s2);
-			if (m1)
-				lo1 = __shfl_sync(FULL, p1, 31 - __clz(m1));
-			if (m2)
-				lo2 = __shfl_sync(FULL, p2, 31 - __clz(m2));
-			bool hit[3] = {false, false, false};
+		uint32_t lo_c = L.c0;
+		warp_intersect2(third, L, [&](bool found, uint32_t x, uint32_t pa, uint32_t pb) {
+			uint32_t q0 = DEAD, q1 = DEAD, q2 = DEAD;
+			bool live = false;
 			if (found)
-				settle_flags(t, q0, q1, q2, S, level, hit);
+			{
+				q0 = itri[pa];
+				q1 = itri[pb];
+				live = !(q0 & DEAD) && !(q1 & DEAD);
+			}
+			const uint32_t fm = __ballot_sync(FULL, live);
+			if (!fm)
+				return;
+			const uint32_t pc = live ? lower_bound32(third, lo_c, L.c1, x) : L.c1;
+			lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
+			bool hit[3] = {false, false, false};
+			// absent from C: that partner died and was compacted away (clique destroyed)
+			if (live && pc < L.c1 && __ldg(third + pc) == x)
+			{
+				q2 = itri[pc];
+				if (!(q2 & DEAD))
+					settle_flags(t, q0, q1, q2, S, level, hit);
+			}
 			const uint32_t qs[3] = {q0, q1, q2};
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
@@ -592,7 +580,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 						atomicOr(err, 1u);
 				}
 			}
-		}
+		});
 	}
 }
 
@@ -692,25 +680,44 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		const uint32_t gwarp = grid_for(c, T, PEEL_THREADS / 32, 16);
 		k_peel_init<<<gscan, PEEL_THREADS, 0, c.stream>>>(K, T, ctl);
 		c.launches++;
+		// Profiling (NUCLEUS34_OPT_PROFILE_PEEL): rounds run as plain launches
+		// with an event after every step; per-step totals go to stderr.
+		const bool profile = (c.opt_flags & NUCLEUS34_OPT_PROFILE_PEEL) != 0;
+		constexpr int PROF_STEPS = 8;
+		static const char *const prof_names[PROF_STEPS] = {"gather_next", "scan_min", "gather",	   "mark",
+														   "debit_thread", "debit_warp", "finalize", "advance"};
 		// One round = a fixed kernel sequence that reads its sizes from ctl.
-		auto launch_round = [&]() {
+		auto launch_round = [&](cudaEvent_t *ev) {
+			auto tick = [&](int j) {
+				if (ev)
+					cudaEventRecord(ev[j], c.stream);
+			};
+			tick(0);
 			k_gather_next<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, F0, F1);
+			tick(1);
 			k_scan_min<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T);
+			tick(2);
 			k_gather<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, F0, F1);
+			tick(3);
 			if (flags)
 			{
 				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.off,
 																   inc.third, inc.tri, 3 * T);
+				tick(4);
 				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off,
 																		   inc.third, inc.tri, S, T);
+				tick(5);
 				k_debit_flags_warp<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off, inc.third,
 																		 inc.tri, S, T);
+				tick(6);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, c.dsrc, c.dE, inc.off,
 																	   inc.third, inc.tri, 3 * T);
+				tick(7);
 			}
 			else
 			{
 				k_mark<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, R, S);
+				tick(4);
 				if (variant == NUCLEUS34_ONDEMAND)
 					k_debit_ondemand<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off, inc.third,
 																		   inc.tri, K, R, S, T);
@@ -718,24 +725,44 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 					k_debit_direct<<<gwarp, PEEL_THREADS, 0, c.stream>>>(
 						ctl, F0, F1, csr.off, csr.ids, reinterpret_cast<const uint4 *>(c.dquds), K, R, S, destroyed,
 						T);
+				tick(5);
+				tick(6);
+				tick(7);
 			}
 			k_advance<<<1, 1, 0, c.stream>>>(ctl);
+			if (ev)
+				cudaEventRecord(ev[PROF_STEPS], c.stream);
 		};
 		const uint32_t per_round = flags ? 8u : 6u;
 		// Rounds are replayed from a CUDA graph of ROUNDS_PER_GRAPH rounds; the
-		// host reads one flag per replay. Rounds after the last one are no-ops.
+		// host reads the control block once per replay. Rounds after the last
+		// one are no-ops.
 		constexpr uint32_t ROUNDS_PER_GRAPH = 16;
 		cudaGraph_t graph = nullptr;
 		cudaGraphExec_t exec = nullptr;
-		bool use_graph = cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+		bool use_graph = !profile && cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
 		if (use_graph)
 		{
 			for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
-				launch_round();
+				launch_round(nullptr);
 			use_graph = cudaStreamEndCapture(c.stream, &graph) == cudaSuccess && graph &&
 						cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
 		}
 		cudaGetLastError();
+		std::vector<cudaEvent_t> events;
+		double prof_ms[PROF_STEPS] = {};
+		if (profile)
+		{
+			events.resize(size_t(ROUNDS_PER_GRAPH) * (PROF_STEPS + 1));
+			for (auto &e : events)
+				cudaEventCreate(&e);
+		}
+		// Compaction of the incidence (death-flag peel only): once the
+		// triangles peeled since the last compaction reach half of the live
+		// ones then, the dead entries are dropped so that later rounds scan
+		// shorter lists.
+		uint64_t live_at_compact = T, peeled_at_compact = 0, compactions = 0;
+		bool compaction_on = flags;
 		// Bounded host loop: every round that is not a no-op peels at least one
 		// triangle, so T + 1 rounds suffice; the bound leaves a wide margin.
 		const uint64_t max_rounds = 2 * T + 4096;
@@ -753,23 +780,70 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			}
 			else
 				for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
-					launch_round();
+					launch_round(profile ? &events[size_t(r) * (PROF_STEPS + 1)] : nullptr);
 			rounds += ROUNDS_PER_GRAPH;
 			c.launches += uint64_t(ROUNDS_PER_GRAPH) * per_round;
-			uint32_t hdone = 0;
+			PeelCtl hc{};
 			if (cudaGetLastError() != cudaSuccess ||
-				cudaMemcpyAsync(&hdone, &ctl->c.done, 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+				cudaMemcpyAsync(&hc, &ctl->c, sizeof(PeelCtl), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
 				cudaStreamSynchronize(c.stream) != cudaSuccess)
 			{
 				rc = fail(NUCLEUS34_E_CUDA, std::string("peel rounds: ") + cudaGetErrorString(cudaGetLastError()));
 				break;
 			}
-			done = hdone != 0;
+			if (profile)
+			{
+				for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
+					for (int j = 0; j < PROF_STEPS; ++j)
+					{
+						float ms = 0;
+						const size_t b = size_t(r) * (PROF_STEPS + 1);
+						if (cudaEventElapsedTime(&ms, events[b + j], events[b + j + 1]) == cudaSuccess)
+							prof_ms[j] += ms;
+					}
+				cudaGetLastError();
+			}
+			done = hc.done != 0;
 			if (!done && rounds > max_rounds)
 			{
 				rc = fail(NUCLEUS34_E_TIMEOUT, "peel did not converge within its round bound");
 				break;
 			}
+			if (!done && compaction_on && hc.peeled < T &&
+				2 * (hc.peeled - peeled_at_compact) >= live_at_compact)
+			{
+				Incidence view = inc; // same arrays; only their contents change
+				uint64_t kept = 0;
+				const int crc = compact_incidence(c, view, &kept);
+				if (crc == NUCLEUS34_E_OOM_BUDGET)
+				{
+					// no room for the temporaries: keep peeling on the full lists
+					compaction_on = false;
+					cudaGetLastError();
+					clear_error();
+				}
+				else if (crc)
+				{
+					rc = crc;
+					break;
+				}
+				else
+				{
+					live_at_compact = T - hc.peeled;
+					peeled_at_compact = hc.peeled;
+					compactions++;
+				}
+			}
+		}
+		for (auto &e : events)
+			cudaEventDestroy(e);
+		if (profile)
+		{
+			std::fprintf(stderr, "[peel-profile] rounds=%llu compactions=%llu", (unsigned long long)rounds,
+						 (unsigned long long)compactions);
+			for (int j = 0; j < PROF_STEPS; ++j)
+				std::fprintf(stderr, " %s=%.1fms", prof_names[j], prof_ms[j]);
+			std::fprintf(stderr, "\n");
 		}
 		if (exec)
 			cudaGraphExecDestroy(exec);

@@ -14,6 +14,10 @@ struct Incidence
 	unsigned long long sum_te_sq = 0; // sum over edges of (list length)^2
 };
 
+// Bit of an incidence entry's tri word that marks a peeled triangle (on-demand
+// peel with death flags; the incidence is discarded after the peel).
+constexpr uint32_t INC_DEAD = 0x80000000u;
+
 // Triangle -> four-clique incidence of the direct variant.
 struct CliqueCsr
 {
@@ -30,6 +34,9 @@ cudaError_t launch_tri_write(const uint32_t *O, const uint32_t *E, uint64_t n, c
 int list_triangles(Ctx &c);
 int build_incidence(Ctx &c, Incidence &inc);
 void free_incidence(Ctx &c, Incidence &inc);
+// Drops the entries marked INC_DEAD from every edge list, in place (same
+// arrays, shorter segments, order kept); *kept = entries left.
+int compact_incidence(Ctx &c, Incidence &inc, uint64_t *kept);
 // support[t] = number of four-cliques on t; returns sum(support) in *total.
 // own (optional): cliques whose lowest triangle is t (direct variant sizes).
 int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total, uint32_t *own);

@@ -7,7 +7,8 @@
 // in atomic order and builds the triangle -> clique incidence by
 // sort_by_key + lower_bound (cuNucleus34.cu:627-669).
 //
-// Here: one warp per triangle runs the 3-way intersection (intersect.cuh).
+// Here: the two shortest incidence lists of each triangle are intersected
+// (intersect.cuh) by one lane (short lists) or one warp (tile merge).
 // Every clique is listed once, by its lowest triangle id, in ascending order of
 // its fourth vertex: a count pass, a scan and a write pass give a
 // deterministic clique order with no sort. The triangle -> clique CSR uses the
@@ -42,18 +43,27 @@ __device__ __forceinline__ TriEdges tri_lists(const uint32_t *__restrict__ tris,
 	return L;
 }
 
-// Hybrid: each warp takes 32 consecutive triangles, one per lane. Lanes whose
-// shortest list is short intersect on their own; the warp then handles the
-// remaining triangles one at a time with all 32 lanes. With WITH_OWN it also
+__device__ __forceinline__ Lists tri_order(const uint32_t *__restrict__ tris, const uint64_t *__restrict__ incO,
+										   uint64_t t)
+{
+	const TriEdges E = tri_lists(tris, incO, t);
+	return order_lists(E.b0, E.e0, E.b1, E.e1, E.b2, E.e2);
+}
+
+// Support count. Each warp takes 32 consecutive triangles, one per lane: a
+// lane whose shortest list is short intersects its two shortest lists alone;
+// the warp then intersects the remaining triangles one at a time (tile merge,
+// or binary search when the lists are very unequal). With WITH_OWN it also
 // counts the cliques whose lowest triangle id is t (the direct variant's
-// clique-list sizes), from the partner ids the intersection located.
+// clique-list sizes); that needs the partner on the longest list too, found
+// by a forward-moving binary search.
 template <bool WITH_OWN>
 __global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__restrict__ tris, uint64_t T,
-														 const uint64_t *__restrict__ incO,
-														 const uint32_t *__restrict__ third,
-														 const uint32_t *__restrict__ itri,
-														 int32_t *__restrict__ support, uint32_t *__restrict__ own,
-														 unsigned long long *__restrict__ total)
+															const uint64_t *__restrict__ incO,
+															const uint32_t *__restrict__ third,
+															const uint32_t *__restrict__ itri,
+															int32_t *__restrict__ support, uint32_t *__restrict__ own,
+															unsigned long long *__restrict__ total)
 {
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
@@ -63,21 +73,21 @@ __global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__re
 	{
 		const uint64_t t = base + lane;
 		const bool valid = t < T;
-		Driver d{};
+		Lists L{};
 		if (valid)
-		{
-			const TriEdges L = tri_lists(tris, incO, t);
-			d = pick_driver(L.b0, L.e0, L.b1, L.e1, L.b2, L.e2);
-		}
-		const bool small = valid && d.ed - d.bd <= THREAD_MODE_MAX;
+			L = tri_order(tris, incO, t);
+		const bool small = valid && L.a1 - L.a0 <= THREAD_MODE_MAX;
 		if (small)
 		{
-			uint32_t cnt = 0, mine = 0;
-			thread_intersect3(third, d, [&](uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
+			uint32_t cnt = 0, mine = 0, lo_c = L.c0;
+			lane_intersect2(third, L, [&](uint32_t x, uint32_t pa, uint32_t pb) {
 				++cnt;
 				if (WITH_OWN)
-					mine += uint32_t(t) < __ldg(itri + pd) && uint32_t(t) < __ldg(itri + p1) &&
-							uint32_t(t) < __ldg(itri + p2);
+				{
+					lo_c = lower_bound32(third, lo_c, L.c1, x);
+					mine += uint32_t(t) < __ldg(itri + pa) && uint32_t(t) < __ldg(itri + pb) &&
+							uint32_t(t) < __ldg(itri + lo_c);
+				}
 			});
 			support[t] = int32_t(cnt);
 			if (WITH_OWN)
@@ -89,22 +99,21 @@ __global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__re
 		{
 			const int j = __ffs(large) - 1;
 			large &= large - 1;
-			const uint64_t tj = base + uint64_t(j);
-			const uint32_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
-			const uint32_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
-			const uint32_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
-			uint32_t cnt = 0, mine = 0;
-			warp_intersect3(third, bd, ed, lo1, hi1, lo2, hi2,
-							[&](bool found, uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
-								cnt += __popc(__ballot_sync(FULL, found));
-								if (WITH_OWN)
-								{
-									const bool m = found && uint32_t(tj) < __ldg(itri + pd) &&
-												   uint32_t(tj) < __ldg(itri + p1) &&
-												   uint32_t(tj) < __ldg(itri + p2);
-									mine += __popc(__ballot_sync(FULL, m));
-								}
-							});
+			const uint32_t tj = uint32_t(base) + uint32_t(j);
+			const Lists Lj{__shfl_sync(FULL, L.a0, j), __shfl_sync(FULL, L.a1, j), __shfl_sync(FULL, L.b0, j),
+						   __shfl_sync(FULL, L.b1, j), __shfl_sync(FULL, L.c0, j), __shfl_sync(FULL, L.c1, j)};
+			uint32_t cnt = 0, mine = 0, lo_c = Lj.c0;
+			warp_intersect2(third, Lj, [&](bool found, uint32_t x, uint32_t pa, uint32_t pb) {
+				const uint32_t fm = __ballot_sync(FULL, found);
+				cnt += __popc(fm);
+				if (WITH_OWN && fm)
+				{
+					const uint32_t pc = found ? lower_bound32(third, lo_c, Lj.c1, x) : Lj.c1;
+					const bool m = found && tj < __ldg(itri + pa) && tj < __ldg(itri + pb) && tj < __ldg(itri + pc);
+					mine += __popc(__ballot_sync(FULL, m));
+					lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
+				}
+			});
 			if (lane == uint32_t(j))
 			{
 				support[tj] = int32_t(cnt);
@@ -146,12 +155,12 @@ __device__ __forceinline__ void sort3(uint32_t &a, uint32_t &b, uint32_t &c)
 
 // Writes each triangle's owned cliques (lowest member t) at qoff[t], in
 // ascending fourth-vertex order; same hybrid thread/warp split as k_support.
-__global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__restrict__ tris, uint64_t T,
-															  const uint64_t *__restrict__ incO,
-															  const uint32_t *__restrict__ third,
-															  const uint32_t *__restrict__ itri,
-															  const uint64_t *__restrict__ qoff,
-															  uint4 *__restrict__ quds)
+__global__ void __launch_bounds__(SUP_THREADS, 4) k_clique_write(const uint32_t *__restrict__ tris, uint64_t T,
+																 const uint64_t *__restrict__ incO,
+																 const uint32_t *__restrict__ third,
+																 const uint32_t *__restrict__ itri,
+																 const uint64_t *__restrict__ qoff,
+																 uint4 *__restrict__ quds)
 {
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
@@ -160,7 +169,7 @@ __global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__
 	{
 		const uint64_t t = base + lane;
 		bool work = false;
-		Driver d{};
+		Lists L{};
 		uint64_t out = 0, out_end = 0;
 		if (t < T)
 		{
@@ -168,16 +177,15 @@ __global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__
 			out_end = qoff[t + 1];
 			work = out < out_end;
 			if (work)
-			{
-				const TriEdges L = tri_lists(tris, incO, t);
-				d = pick_driver(L.b0, L.e0, L.b1, L.e1, L.b2, L.e2);
-			}
+				L = tri_order(tris, incO, t);
 		}
-		const bool small = work && d.ed - d.bd <= THREAD_MODE_MAX;
+		const bool small = work && L.a1 - L.a0 <= THREAD_MODE_MAX;
 		if (small)
 		{
-			thread_intersect3(third, d, [&](uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
-				uint32_t q0 = __ldg(itri + pd), q1 = __ldg(itri + p1), q2 = __ldg(itri + p2);
+			uint32_t lo_c = L.c0;
+			lane_intersect2(third, L, [&](uint32_t x, uint32_t pa, uint32_t pb) {
+				lo_c = lower_bound32(third, lo_c, L.c1, x);
+				uint32_t q0 = __ldg(itri + pa), q1 = __ldg(itri + pb), q2 = __ldg(itri + lo_c);
 				if (uint32_t(t) < q0 && uint32_t(t) < q1 && uint32_t(t) < q2 && out < out_end)
 				{
 					sort3(q0, q1, q2);
@@ -193,29 +201,33 @@ __global__ void __launch_bounds__(SUP_THREADS) k_clique_write(const uint32_t *__
 			const uint32_t tj = uint32_t(base) + uint32_t(j);
 			uint64_t o = __shfl_sync(FULL, out, j);
 			const uint64_t oe = __shfl_sync(FULL, out_end, j);
-			const uint32_t bd = __shfl_sync(FULL, d.bd, j), ed = __shfl_sync(FULL, d.ed, j);
-			const uint32_t lo1 = __shfl_sync(FULL, d.lo1, j), hi1 = __shfl_sync(FULL, d.hi1, j);
-			const uint32_t lo2 = __shfl_sync(FULL, d.lo2, j), hi2 = __shfl_sync(FULL, d.hi2, j);
-			warp_intersect3(third, bd, ed, lo1, hi1, lo2, hi2,
-							[&](bool found, uint32_t, uint32_t pd, uint32_t p1, uint32_t p2) {
-								bool mine = false;
-								uint32_t q0 = 0, q1 = 0, q2 = 0;
-								if (found)
-								{
-									q0 = __ldg(itri + pd);
-									q1 = __ldg(itri + p1);
-									q2 = __ldg(itri + p2);
-									mine = tj < q0 && tj < q1 && tj < q2;
-								}
-								const uint32_t word = __ballot_sync(FULL, mine);
-								const uint64_t at = o + __popc(word & lanemask_lt());
-								if (mine && at < oe) // capacity guard (the count pass sized it)
-								{
-									sort3(q0, q1, q2);
-									quds[at] = make_uint4(tj, q0, q1, q2);
-								}
-								o += __popc(word);
-							});
+			const Lists Lj{__shfl_sync(FULL, L.a0, j), __shfl_sync(FULL, L.a1, j), __shfl_sync(FULL, L.b0, j),
+						   __shfl_sync(FULL, L.b1, j), __shfl_sync(FULL, L.c0, j), __shfl_sync(FULL, L.c1, j)};
+			uint32_t lo_c = Lj.c0;
+			warp_intersect2(third, Lj, [&](bool found, uint32_t x, uint32_t pa, uint32_t pb) {
+				const uint32_t fm = __ballot_sync(FULL, found);
+				if (!fm)
+					return;
+				const uint32_t pc = found ? lower_bound32(third, lo_c, Lj.c1, x) : Lj.c1;
+				lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
+				uint32_t q0 = 0, q1 = 0, q2 = 0;
+				bool mine = false;
+				if (found)
+				{
+					q0 = __ldg(itri + pa);
+					q1 = __ldg(itri + pb);
+					q2 = __ldg(itri + pc);
+					mine = tj < q0 && tj < q1 && tj < q2;
+				}
+				const uint32_t word = __ballot_sync(FULL, mine);
+				const uint64_t at = o + __popc(word & lanemask_lt());
+				if (mine && at < oe) // capacity guard (the count pass sized it)
+				{
+					sort3(q0, q1, q2);
+					quds[at] = make_uint4(tj, q0, q1, q2);
+				}
+				o += __popc(word);
+			});
 		}
 	}
 }

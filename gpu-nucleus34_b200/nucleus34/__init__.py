@@ -275,6 +275,7 @@ class Decomposition:
 
 
 OPT_STAMP_PEEL = 0x1
+OPT_PROFILE_PEEL = 0x2
 
 
 def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1, flags: int = 0) -> Opts:

@@ -77,6 +77,10 @@ typedef struct
 /* opts.flags: force the round-stamp ownership test in the on-demand peel
  * (the default keeps death flags inside the incidence entries when T < 2^30). */
 #define NUCLEUS34_OPT_STAMP_PEEL 0x1u
+/* opts.flags: run the peel rounds as plain launches with CUDA events around
+ * every step and print per-step device times to stderr (diagnostics only;
+ * slower than the default graph replay). */
+#define NUCLEUS34_OPT_PROFILE_PEEL 0x2u
 
 typedef struct
 {
