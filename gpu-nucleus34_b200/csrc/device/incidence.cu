@@ -243,11 +243,15 @@ __global__ void k_alive_count(const uint64_t *__restrict__ off, uint64_t m, cons
 }
 
 // Stable per-edge copy of the live entries into their new segment (order by
-// third vertex is kept, so every list stays sorted).
+// third vertex is kept, so every list stays sorted). Writes stop at cap (the
+// caller's bound on live entries); a count beyond it sets *err.
 __global__ void k_compact_copy(const uint64_t *__restrict__ off, const uint64_t *__restrict__ noff, uint64_t m,
 							   const uint32_t *__restrict__ third, const uint32_t *__restrict__ tri,
-							   uint32_t *__restrict__ third2, uint32_t *__restrict__ tri2)
+							   uint32_t *__restrict__ third2, uint32_t *__restrict__ tri2, uint64_t cap,
+							   uint32_t *__restrict__ err)
 {
+	if (blockIdx.x == 0 && threadIdx.x == 0 && noff[m] > cap)
+		atomicOr(err, 2u);
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
 	const uint32_t lane = lane_id();
@@ -269,11 +273,33 @@ __global__ void k_compact_copy(const uint64_t *__restrict__ off, const uint64_t 
 			if (keep)
 			{
 				const uint64_t o = out + __popc(bal & ((1u << lane) - 1u));
-				third2[o] = x;
-				tri2[o] = t;
+				if (o < cap)
+				{
+					third2[o] = x;
+					tri2[o] = t;
+				}
 			}
 			out += __popc(bal);
 		}
+	}
+}
+
+// Copies the compacted lists (noff[m] entries, at most cap) and offsets back.
+__global__ void k_compact_back(const uint64_t *__restrict__ noff, uint64_t m, const uint32_t *__restrict__ third2,
+							   const uint32_t *__restrict__ tri2, uint64_t cap, uint64_t *__restrict__ off,
+							   uint32_t *__restrict__ third, uint32_t *__restrict__ tri)
+{
+	const uint64_t n = noff[m] < cap ? noff[m] : cap;
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n || i <= m; i += stride)
+	{
+		if (i < n)
+		{
+			third[i] = third2[i];
+			tri[i] = tri2[i];
+		}
+		if (i <= m)
+			off[i] = noff[i];
 	}
 }
 
@@ -403,54 +429,38 @@ int build_incidence(Ctx &c, Incidence &inc)
 	return rc;
 }
 
-int compact_incidence(Ctx &c, Incidence &inc, uint64_t *kept)
+int compact_incidence(Ctx &c, Incidence &inc, uint64_t cap, uint32_t *err)
 {
-	const uint64_t m = c.m, n3 = 3 * c.T;
+	const uint64_t m = c.m;
 	uint32_t *cnt = nullptr, *third2 = nullptr, *tri2 = nullptr;
 	uint64_t *noff = nullptr;
 	int rc = NUCLEUS34_OK;
 	do
 	{
+		if (cap > 3 * c.T)
+			cap = 3 * c.T;
 		if ((rc = dalloc(c, &cnt, m ? m : 1, "compaction counts")))
 			break;
 		if ((rc = dalloc(c, &noff, m + 1, "compaction offsets")))
+			break;
+		if ((rc = dalloc(c, &third2, cap ? cap : 1, "compaction third")))
+			break;
+		if ((rc = dalloc(c, &tri2, cap ? cap : 1, "compaction tri")))
 			break;
 		const uint32_t gw = grid_for(c, m, 256 / 32, 16);
 		k_alive_count<<<gw, 256, 0, c.stream>>>(inc.off, m, inc.tri, cnt);
 		c.launches++;
 		if ((rc = scan_u32(c, cnt, noff, m)))
 			break;
-		uint64_t live = 0;
-		if (cudaMemcpyAsync(&live, noff + m, 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
-			cudaStreamSynchronize(c.stream) != cudaSuccess)
-		{
-			rc = fail(NUCLEUS34_E_CUDA, "compaction count");
-			break;
-		}
-		if (live > n3)
-		{
-			rc = fail(NUCLEUS34_E_CUDA, "internal: compaction count");
-			break;
-		}
-		const uint64_t cap = live ? live : 1;
-		if ((rc = dalloc(c, &third2, cap, "compaction third")))
-			break;
-		if ((rc = dalloc(c, &tri2, cap, "compaction tri")))
-			break;
-		k_compact_copy<<<gw, 256, 0, c.stream>>>(inc.off, noff, m, inc.third, inc.tri, third2, tri2);
+		k_compact_copy<<<gw, 256, 0, c.stream>>>(inc.off, noff, m, inc.third, inc.tri, third2, tri2, cap, err);
 		c.launches++;
-		// Copy back into the same arrays so that kernels captured with these
-		// pointers stay valid.
-		if ((live && (cudaMemcpyAsync(inc.third, third2, live * 4, cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess ||
-					  cudaMemcpyAsync(inc.tri, tri2, live * 4, cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess)) ||
-			cudaMemcpyAsync(inc.off, noff, (m + 1) * 8, cudaMemcpyDeviceToDevice, c.stream) != cudaSuccess ||
-			cudaGetLastError() != cudaSuccess)
-		{
-			rc = fail(NUCLEUS34_E_CUDA, "compaction copy");
-			break;
-		}
-		if (kept)
-			*kept = live;
+		// Back into the same arrays (kernels captured with these pointers stay
+		// valid); the live count is read on the device, so nothing waits here.
+		k_compact_back<<<grid_for(c, cap > m + 1 ? cap : m + 1, 256), 256, 0, c.stream>>>(noff, m, third2, tri2, cap,
+																						   inc.off, inc.third, inc.tri);
+		c.launches++;
+		if (cudaGetLastError() != cudaSuccess)
+			rc = fail(NUCLEUS34_E_CUDA, "compaction kernels");
 	} while (false);
 	c.release(cnt);
 	c.release(noff);

@@ -58,18 +58,71 @@ __device__ __forceinline__ Lists order_lists(uint32_t x0, uint32_t x1, uint32_t 
 constexpr uint32_t THREAD_MODE_MAX = 16;
 // B longer than this multiple of A: binary-search B instead of merging.
 constexpr uint32_t MERGE_RATIO = 24;
+// Search ranges at least this long start with a warp-wide sample of 32
+// evenly spaced entries (one round trip instead of five halvings).
+#ifndef N34_SAMPLE_MIN
+#define N34_SAMPLE_MIN 256u
+#endif
 
 __device__ __forceinline__ bool use_merge(const Lists &L)
 {
 	return (L.b1 - L.b0) <= MERGE_RATIO * (L.a1 - L.a0);
 }
 
-// Warp tile merge of A and B. f(found, x, pa, pb) is called by all lanes once
-// per step; found lanes hold x = third[pa] = third[pb]. Each common x is seen
-// exactly once, in ascending order across steps.
-template <class F>
-__device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, uint32_t a0, uint32_t a1, uint32_t b0,
-											uint32_t b1, F &&f)
+// Warp lower bounds: every lane with want gets the first position in [lo, hi)
+// whose entry is >= its x (hi if none). Called by all lanes. Long ranges are
+// first narrowed to 1/32 by a sample of 32 evenly spaced entries loaded at
+// once, so the per-lane binary searches start five levels down.
+__device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi,
+													 bool want, uint32_t x)
+{
+	const uint32_t n = hi - lo;
+	uint32_t l = lo, h = hi;
+	if (n >= N34_SAMPLE_MIN) // warp-uniform
+	{
+		const uint32_t lane = lane_id();
+		// sample i sits at the end of slice i: lo + ceil(n * (i+1) / 32) - 1
+		const uint32_t sp = lo + uint32_t((uint64_t(n) * (lane + 1) + 31) >> 5) - 1;
+		const uint32_t sv = __ldg(a + sp);
+		// first sample >= x (32 if none)
+		uint32_t j = 0;
+#pragma unroll
+		for (uint32_t step = 16; step > 0; step >>= 1)
+		{
+			const uint32_t probe = __shfl_sync(FULL, sv, (j + step - 1) & 31);
+			if (probe < x)
+				j += step;
+		}
+		const uint32_t last = __shfl_sync(FULL, sv, 31);
+		const uint32_t sj = __shfl_sync(FULL, sp, j & 31);
+		const uint32_t sprev = __shfl_sync(FULL, sp, (j + 31) & 31);
+		if (last < x)
+		{
+			l = hi;
+			h = hi;
+		}
+		else
+		{
+			l = j ? sprev + 1 : lo;
+			h = sj; // a[sj] >= x: the bound is at most sj
+		}
+	}
+	uint32_t r = hi;
+	if (want)
+	{
+		r = lower_bound32(a, l, h, x);
+	}
+	return r;
+}
+
+// Warp tile merge of A and B. f(found, x, pa, pb, qa, qb) is called by all
+// lanes once per step; found lanes hold x = third[pa] = third[pb], and with
+// WITH_TRI also qa = itri[pa], qb = itri[pb] (the partner tiles are loaded
+// together with the third tiles, saving a dependent round trip). Each common
+// x is seen exactly once, in ascending order across steps.
+template <bool WITH_TRI, class F>
+__device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
+											uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, F &&f)
 {
 	const uint32_t lane = lane_id();
 	while (a0 < a1 && b0 < b1) // warp-uniform
@@ -78,6 +131,12 @@ __device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, 
 		const bool av_ok = ai < a1, bv_ok = bi < b1;
 		const uint32_t av = av_ok ? __ldg(third + ai) : 0xffffffffu;
 		const uint32_t bv = bv_ok ? __ldg(third + bi) : 0xffffffffu;
+		uint32_t at = 0, bt = 0;
+		if (WITH_TRI)
+		{
+			at = av_ok ? __ldg(itri + ai) : 0u;
+			bt = bv_ok ? __ldg(itri + bi) : 0u;
+		}
 		const uint32_t amax = __shfl_sync(FULL, av, 31), bmax = __shfl_sync(FULL, bv, 31);
 		const uint32_t m = amax < bmax ? amax : bmax;
 		// first lane j of the B tile with bv_j >= av (31 if none: then no match)
@@ -90,8 +149,9 @@ __device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, 
 				pos += step;
 		}
 		const uint32_t hitv = __shfl_sync(FULL, bv, pos & 31);
+		const uint32_t qb = WITH_TRI ? __shfl_sync(FULL, bt, pos & 31) : 0u;
 		const bool found = av_ok && av <= m && hitv == av && b0 + pos < b1;
-		f(found, av, ai, b0 + pos);
+		f(found, av, ai, b0 + pos, at, qb);
 		// everything <= m is consumed; at least one tile is used up entirely
 		a0 += __popc(__ballot_sync(FULL, av_ok && av <= m));
 		b0 += __popc(__ballot_sync(FULL, bv_ok && bv <= m));
@@ -99,9 +159,9 @@ __device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, 
 }
 
 // Warp binary search of A's entries in B (B much longer than A).
-template <class F>
-__device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third, uint32_t a0, uint32_t a1, uint32_t b0,
-											 uint32_t b1, F &&f)
+template <bool WITH_TRI, class F>
+__device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
+											 uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, F &&f)
 {
 	const uint32_t lane = lane_id();
 	for (uint32_t base = a0; base < a1; base += 32)
@@ -111,11 +171,11 @@ __device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third,
 		const uint32_t ai = base + lane;
 		const bool ok = ai < a1;
 		const uint32_t x = ok ? __ldg(third + ai) : 0xffffffffu;
-		uint32_t p = b1;
-		if (ok)
-			p = lower_bound32(third, b0, b1, x);
+		const uint32_t at = (WITH_TRI && ok) ? __ldg(itri + ai) : 0u;
+		const uint32_t p = warp_lower_bound(third, b0, b1, ok, x);
 		const bool found = ok && p < b1 && __ldg(third + p) == x;
-		f(found, x, ai, p);
+		const uint32_t bt = (WITH_TRI && found) ? __ldg(itri + p) : 0u;
+		f(found, x, ai, p, at, bt);
 		// later steps hold larger x: the highest searching lane's bound stays valid
 		const uint32_t msk = __ballot_sync(FULL, ok);
 		b0 = __shfl_sync(FULL, p, 31 - __clz(msk));
@@ -123,13 +183,14 @@ __device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third,
 }
 
 // Warp dispatch between merge and search for the two shortest lists.
-template <class F>
-__device__ __forceinline__ void warp_intersect2(const uint32_t *__restrict__ third, const Lists &L, F &&f)
+template <bool WITH_TRI = false, class F>
+__device__ __forceinline__ void warp_intersect2(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
+												const Lists &L, F &&f)
 {
 	if (use_merge(L))
-		warp_merge2(third, L.a0, L.a1, L.b0, L.b1, f);
+		warp_merge2<WITH_TRI>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
 	else
-		warp_search2(third, L.a0, L.a1, L.b0, L.b1, f);
+		warp_search2<WITH_TRI>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
 }
 
 // One lane on its own: each entry of A binary-searched in B (the window only

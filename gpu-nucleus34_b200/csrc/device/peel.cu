@@ -37,6 +37,9 @@ namespace {
 
 constexpr uint32_t INF = 0xffffffffu;
 constexpr int PEEL_THREADS = 256;
+#ifndef N34_COMPACT_DIV
+#define N34_COMPACT_DIV 8
+#endif
 
 struct CtlX
 {
@@ -261,17 +264,19 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_ondemand(
 		const uint32_t t = F[i];
 		const Lists L = frontier_lists(t, tris, incO);
 		uint32_t lo_c = L.c0;
-		warp_intersect2(third, L, [&](bool found, uint32_t x, uint32_t pa, uint32_t pb) {
+		warp_intersect2<true>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
+												  uint32_t qb) {
 			const uint32_t fm = __ballot_sync(FULL, found);
 			if (!fm)
 				return;
-			const uint32_t pc = found ? lower_bound32(third, lo_c, L.c1, x) : L.c1;
+			const uint32_t pc = warp_lower_bound(third, lo_c, L.c1, found, x);
 			lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
+			found = found && pc < L.c1; // always true without compaction
 			uint32_t q0 = 0, q1 = 0, q2 = 0;
 			if (found)
 			{
-				q0 = __ldg(itri + pa);
-				q1 = __ldg(itri + pb);
+				q0 = qa;
+				q1 = qb;
 				q2 = __ldg(itri + pc);
 			}
 			settle_clique(found, t, q0, q1, q2, K, R, S, round, level, Fn, &ctl->c.nNext, T, &ctl->c.error);
@@ -485,7 +490,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 		uint32_t lo_b = L.b0, lo_c = L.c0;
 		for (uint32_t i = L.a0; i < L.a1 && lo_b < L.b1; ++i)
 		{
-			const uint32_t q0 = itri[i];
+			const uint32_t q0 = __ldg(itri + i);
 			if (q0 & DEAD)
 				continue;
 			const uint32_t x = __ldg(third + i);
@@ -494,13 +499,13 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 				break;
 			if (__ldg(third + lo_b) != x)
 				continue;
-			const uint32_t q1 = itri[lo_b];
+			const uint32_t q1 = __ldg(itri + lo_b);
 			if (q1 & DEAD)
 				continue;
 			lo_c = lower_bound32(third, lo_c, L.c1, x);
 			if (lo_c >= L.c1 || __ldg(third + lo_c) != x)
 				continue; // the partner on the longest list was compacted away
-			const uint32_t q2 = itri[lo_c];
+			const uint32_t q2 = __ldg(itri + lo_c);
 			if (q2 & DEAD)
 				continue;
 			bool hit[3];
@@ -545,25 +550,26 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 		if (L.a1 - L.a0 <= THREAD_MODE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
 		uint32_t lo_c = L.c0;
-		warp_intersect2(third, L, [&](bool found, uint32_t x, uint32_t pa, uint32_t pb) {
+		warp_intersect2<true>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
+												  uint32_t qb) {
 			uint32_t q0 = DEAD, q1 = DEAD, q2 = DEAD;
 			bool live = false;
 			if (found)
 			{
-				q0 = itri[pa];
-				q1 = itri[pb];
+				q0 = qa;
+				q1 = qb;
 				live = !(q0 & DEAD) && !(q1 & DEAD);
 			}
 			const uint32_t fm = __ballot_sync(FULL, live);
 			if (!fm)
 				return;
-			const uint32_t pc = live ? lower_bound32(third, lo_c, L.c1, x) : L.c1;
+			const uint32_t pc = warp_lower_bound(third, lo_c, L.c1, live, x);
 			lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
 			bool hit[3] = {false, false, false};
 			// absent from C: that partner died and was compacted away (clique destroyed)
 			if (live && pc < L.c1 && __ldg(third + pc) == x)
 			{
-				q2 = itri[pc];
+				q2 = __ldg(itri + pc);
 				if (!(q2 & DEAD))
 					settle_flags(t, q0, q1, q2, S, level, hit);
 			}
@@ -687,7 +693,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		static const char *const prof_names[PROF_STEPS] = {"gather_next", "scan_min", "gather",	   "mark",
 														   "debit_thread", "debit_warp", "finalize", "advance"};
 		// One round = a fixed kernel sequence that reads its sizes from ctl.
-		auto launch_round = [&](cudaEvent_t *ev) {
+		auto launch_round = [&](cudaEvent_t *ev, uint32_t *trace) {
 			auto tick = [&](int j) {
 				if (ev)
 					cudaEventRecord(ev[j], c.stream);
@@ -699,6 +705,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			tick(2);
 			k_gather<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, F0, F1);
 			tick(3);
+			if (trace)
+				cudaMemcpyAsync(trace, &ctl->c, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream);
 			if (flags)
 			{
 				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.off,
@@ -744,77 +752,118 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		if (use_graph)
 		{
 			for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
-				launch_round(nullptr);
+				launch_round(nullptr, nullptr);
 			use_graph = cudaStreamEndCapture(c.stream, &graph) == cudaSuccess && graph &&
 						cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
 		}
 		cudaGetLastError();
 		std::vector<cudaEvent_t> events;
 		double prof_ms[PROF_STEPS] = {};
+		uint32_t *trace_buf = nullptr; // (level, round, frontier size) per round
 		if (profile)
 		{
+			if (cudaMallocHost(&trace_buf, 3 * sizeof(uint32_t) * ROUNDS_PER_GRAPH) != cudaSuccess)
+			{
+				trace_buf = nullptr; // profile without the per-round lines
+				cudaGetLastError();
+			}
 			events.resize(size_t(ROUNDS_PER_GRAPH) * (PROF_STEPS + 1));
 			for (auto &e : events)
 				cudaEventCreate(&e);
 		}
 		// Compaction of the incidence (death-flag peel only): once the
-		// triangles peeled since the last compaction reach half of the live
-		// ones then, the dead entries are dropped so that later rounds scan
-		// shorter lists.
+		// triangles peeled since the last compaction reach 1/N34_COMPACT_DIV
+		// of the live ones then, the dead entries are dropped so that later
+		// rounds scan shorter lists. A compaction costs one pass over the live
+		// entries, so the passes form a geometric series (at most
+		// N34_COMPACT_DIV passes over the full incidence in total).
 		uint64_t live_at_compact = T, peeled_at_compact = 0, compactions = 0;
 		bool compaction_on = flags;
 		// Bounded host loop: every round that is not a no-op peels at least one
 		// triangle, so T + 1 rounds suffice; the bound leaves a wide margin.
+		// The next replay is queued before the host reads the control block of
+		// the previous one (pinned ring of two), so the GPU never waits on the
+		// host; after the last round the queued replay is all no-ops.
 		const uint64_t max_rounds = 2 * T + 4096;
 		uint64_t rounds = 0;
-		bool done = false;
-		while (!done)
-		{
+		PeelCtl *ring = nullptr;
+		cudaEvent_t ring_ev[2] = {nullptr, nullptr};
+		if (cudaMallocHost(&ring, 2 * sizeof(PeelCtl)) != cudaSuccess ||
+			cudaEventCreateWithFlags(&ring_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+			cudaEventCreateWithFlags(&ring_ev[1], cudaEventDisableTiming) != cudaSuccess)
+			rc = fail(NUCLEUS34_E_CUDA, "peel control ring");
+		auto enqueue = [&](int slot) -> bool {
 			if (use_graph)
 			{
 				if (cudaGraphLaunch(exec, c.stream) != cudaSuccess)
-				{
-					rc = fail(NUCLEUS34_E_CUDA, "peel graph launch");
-					break;
-				}
+					return false;
 			}
 			else
 				for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
-					launch_round(profile ? &events[size_t(r) * (PROF_STEPS + 1)] : nullptr);
+					launch_round(profile ? &events[size_t(r) * (PROF_STEPS + 1)] : nullptr,
+								 trace_buf ? trace_buf + 3 * r : nullptr);
 			rounds += ROUNDS_PER_GRAPH;
 			c.launches += uint64_t(ROUNDS_PER_GRAPH) * per_round;
-			PeelCtl hc{};
-			if (cudaGetLastError() != cudaSuccess ||
-				cudaMemcpyAsync(&hc, &ctl->c, sizeof(PeelCtl), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
-				cudaStreamSynchronize(c.stream) != cudaSuccess)
+			return cudaMemcpyAsync(&ring[slot], &ctl->c, sizeof(PeelCtl), cudaMemcpyDeviceToHost, c.stream) ==
+					   cudaSuccess &&
+				   cudaEventRecord(ring_ev[slot], c.stream) == cudaSuccess;
+		};
+		// profiling reads per-round events, so it runs one replay at a time
+		const int depth = profile ? 1 : 2;
+		uint64_t issued = 0, consumed = 0;
+		while (!rc && issued < uint64_t(depth))
+		{
+			if (!enqueue(int(issued & 1)))
+				rc = fail(NUCLEUS34_E_CUDA, "peel replay launch");
+			++issued;
+		}
+		while (!rc)
+		{
+			const int slot = int(consumed & 1);
+			if (cudaEventSynchronize(ring_ev[slot]) != cudaSuccess || cudaGetLastError() != cudaSuccess)
 			{
 				rc = fail(NUCLEUS34_E_CUDA, std::string("peel rounds: ") + cudaGetErrorString(cudaGetLastError()));
 				break;
 			}
+			const PeelCtl hc = ring[slot];
+			++consumed;
 			if (profile)
 			{
 				for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
+				{
+					const uint32_t *tr = trace_buf ? trace_buf + 3 * r : nullptr;
+					if (tr && !tr[2])
+						continue; // no-op round
+					if (tr)
+						std::fprintf(stderr, "[peel-round] level=%u round=%u frontier=%u", tr[0], tr[1], tr[2]);
 					for (int j = 0; j < PROF_STEPS; ++j)
 					{
 						float ms = 0;
 						const size_t b = size_t(r) * (PROF_STEPS + 1);
 						if (cudaEventElapsedTime(&ms, events[b + j], events[b + j + 1]) == cudaSuccess)
 							prof_ms[j] += ms;
+						if (tr)
+							std::fprintf(stderr, " %.3f", ms);
 					}
+					if (tr)
+						std::fprintf(stderr, "\n");
+				}
 				cudaGetLastError();
 			}
-			done = hc.done != 0;
-			if (!done && rounds > max_rounds)
+			if (hc.done)
+				break;
+			if (rounds > max_rounds)
 			{
 				rc = fail(NUCLEUS34_E_TIMEOUT, "peel did not converge within its round bound");
 				break;
 			}
-			if (!done && compaction_on && hc.peeled < T &&
-				2 * (hc.peeled - peeled_at_compact) >= live_at_compact)
+			if (compaction_on && hc.peeled < T &&
+				N34_COMPACT_DIV * (hc.peeled - peeled_at_compact) >= live_at_compact)
 			{
+				// queued behind the replay in flight, when no fewer triangles are
+				// peeled: 3 entries per live triangle bound the live entries
 				Incidence view = inc; // same arrays; only their contents change
-				uint64_t kept = 0;
-				const int crc = compact_incidence(c, view, &kept);
+				const int crc = compact_incidence(c, view, 3 * (T - hc.peeled), &ctl->c.error);
 				if (crc == NUCLEUS34_E_OOM_BUDGET)
 				{
 					// no room for the temporaries: keep peeling on the full lists
@@ -834,9 +883,25 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 					compactions++;
 				}
 			}
+			if (!enqueue(int(issued & 1)))
+			{
+				rc = fail(NUCLEUS34_E_CUDA, "peel replay launch");
+				break;
+			}
+			++issued;
 		}
+		// the replay still queued (no-op rounds) completes before the stats
+		if (cudaStreamSynchronize(c.stream) != cudaSuccess && !rc)
+			rc = fail(NUCLEUS34_E_CUDA, "peel drain");
+		for (auto &e : ring_ev)
+			if (e)
+				cudaEventDestroy(e);
+		if (ring)
+			cudaFreeHost(ring);
 		for (auto &e : events)
 			cudaEventDestroy(e);
+		if (trace_buf)
+			cudaFreeHost(trace_buf);
 		if (profile)
 		{
 			std::fprintf(stderr, "[peel-profile] rounds=%llu compactions=%llu", (unsigned long long)rounds,
@@ -861,7 +926,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		}
 		if (hctl->error)
 		{
-			rc = fail(NUCLEUS34_E_CUDA, "internal: peel frontier overflow");
+			rc = fail(NUCLEUS34_E_CUDA, "internal: peel check failed (" +
+									   std::string(hctl->error & 2u ? "compaction bound" : "frontier overflow") + ")");
 			break;
 		}
 	} while (false);

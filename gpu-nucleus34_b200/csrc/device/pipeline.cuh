@@ -35,8 +35,10 @@ int list_triangles(Ctx &c);
 int build_incidence(Ctx &c, Incidence &inc);
 void free_incidence(Ctx &c, Incidence &inc);
 // Drops the entries marked INC_DEAD from every edge list, in place (same
-// arrays, shorter segments, order kept); *kept = entries left.
-int compact_incidence(Ctx &c, Incidence &inc, uint64_t *kept);
+// arrays, shorter segments, order kept), stream-ordered and without waiting
+// on the host. cap bounds the live entries (3 per live triangle); a larger
+// count sets bit 2 in *err and the copy stops at cap.
+int compact_incidence(Ctx &c, Incidence &inc, uint64_t cap, uint32_t *err);
 // support[t] = number of four-cliques on t; returns sum(support) in *total.
 // own (optional): cliques whose lowest triangle is t (direct variant sizes).
 int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total, uint32_t *own);

@@ -103,15 +103,20 @@ __global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__re
 			const Lists Lj{__shfl_sync(FULL, L.a0, j), __shfl_sync(FULL, L.a1, j), __shfl_sync(FULL, L.b0, j),
 						   __shfl_sync(FULL, L.b1, j), __shfl_sync(FULL, L.c0, j), __shfl_sync(FULL, L.c1, j)};
 			uint32_t cnt = 0, mine = 0, lo_c = Lj.c0;
-			warp_intersect2(third, Lj, [&](bool found, uint32_t x, uint32_t pa, uint32_t pb) {
+			warp_intersect2<WITH_OWN>(third, itri, Lj, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
+														   uint32_t qb) {
 				const uint32_t fm = __ballot_sync(FULL, found);
 				cnt += __popc(fm);
 				if (WITH_OWN && fm)
 				{
-					const uint32_t pc = found ? lower_bound32(third, lo_c, Lj.c1, x) : Lj.c1;
-					const bool m = found && tj < __ldg(itri + pa) && tj < __ldg(itri + pb) && tj < __ldg(itri + pc);
+					// the longest list is searched only where t is below the other two
+					const bool cand = found && tj < qa && tj < qb;
+					const uint32_t pc = warp_lower_bound(third, lo_c, Lj.c1, cand, x);
+					const bool m = cand && pc < Lj.c1 && tj < __ldg(itri + pc);
 					mine += __popc(__ballot_sync(FULL, m));
-					lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
+					const uint32_t cm = __ballot_sync(FULL, cand);
+					if (cm)
+						lo_c = __shfl_sync(FULL, pc, 31 - __clz(cm));
 				}
 			});
 			if (lane == uint32_t(j))
@@ -204,20 +209,21 @@ __global__ void __launch_bounds__(SUP_THREADS, 4) k_clique_write(const uint32_t 
 			const Lists Lj{__shfl_sync(FULL, L.a0, j), __shfl_sync(FULL, L.a1, j), __shfl_sync(FULL, L.b0, j),
 						   __shfl_sync(FULL, L.b1, j), __shfl_sync(FULL, L.c0, j), __shfl_sync(FULL, L.c1, j)};
 			uint32_t lo_c = Lj.c0;
-			warp_intersect2(third, Lj, [&](bool found, uint32_t x, uint32_t pa, uint32_t pb) {
-				const uint32_t fm = __ballot_sync(FULL, found);
-				if (!fm)
+			warp_intersect2<true>(third, itri, Lj, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
+													   uint32_t qb) {
+				// the longest list is searched only where t is below the other two
+				const bool cand = found && tj < qa && tj < qb;
+				const uint32_t cm = __ballot_sync(FULL, cand);
+				if (!cm)
 					return;
-				const uint32_t pc = found ? lower_bound32(third, lo_c, Lj.c1, x) : Lj.c1;
-				lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
-				uint32_t q0 = 0, q1 = 0, q2 = 0;
+				const uint32_t pc = warp_lower_bound(third, lo_c, Lj.c1, cand, x);
+				lo_c = __shfl_sync(FULL, pc, 31 - __clz(cm));
+				uint32_t q0 = qa, q1 = qb, q2 = 0;
 				bool mine = false;
-				if (found)
+				if (cand && pc < Lj.c1)
 				{
-					q0 = __ldg(itri + pa);
-					q1 = __ldg(itri + pb);
 					q2 = __ldg(itri + pc);
-					mine = tj < q0 && tj < q1 && tj < q2;
+					mine = tj < q2;
 				}
 				const uint32_t word = __ballot_sync(FULL, mine);
 				const uint64_t at = o + __popc(word & lanemask_lt());
