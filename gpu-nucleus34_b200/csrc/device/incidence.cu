@@ -221,86 +221,12 @@ __global__ void k_inc_split(const unsigned long long *__restrict__ keys, uint64_
 	}
 }
 
-// Live entries per edge (warp per edge, coalesced reads of the tri column).
-__global__ void k_alive_count(const uint64_t *__restrict__ off, uint64_t m, const uint32_t *__restrict__ tri,
-							  uint32_t *__restrict__ cnt)
+// Per-edge list bounds as 32-bit (begin, end) pairs (3T < 2^32 entries).
+__global__ void k_make_spans(const uint64_t *__restrict__ off, uint64_t m, uint2 *__restrict__ span)
 {
-	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-	const uint32_t lane = lane_id();
-	for (uint64_t e = warp; e < m; e += nwarps)
-	{
-		const uint64_t b = off[e], en = off[e + 1];
-		uint32_t live = 0;
-		for (uint64_t i = b + lane; i < en; i += 32)
-			live += !(tri[i] & INC_DEAD);
-#pragma unroll
-		for (int o = 16; o > 0; o >>= 1)
-			live += __shfl_xor_sync(FULL, live, o);
-		if (lane == 0)
-			cnt[e] = live;
-	}
-}
-
-// Stable per-edge copy of the live entries into their new segment (order by
-// third vertex is kept, so every list stays sorted). Writes stop at cap (the
-// caller's bound on live entries); a count beyond it sets *err.
-__global__ void k_compact_copy(const uint64_t *__restrict__ off, const uint64_t *__restrict__ noff, uint64_t m,
-							   const uint32_t *__restrict__ third, const uint32_t *__restrict__ tri,
-							   uint32_t *__restrict__ third2, uint32_t *__restrict__ tri2, uint64_t cap,
-							   uint32_t *__restrict__ err)
-{
-	if (blockIdx.x == 0 && threadIdx.x == 0 && noff[m] > cap)
-		atomicOr(err, 2u);
-	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-	const uint32_t lane = lane_id();
-	for (uint64_t e = warp; e < m; e += nwarps)
-	{
-		const uint64_t b = off[e], en = off[e + 1];
-		uint64_t out = noff[e];
-		for (uint64_t base = b; base < en; base += 32)
-		{
-			const uint64_t i = base + lane;
-			uint32_t t = INC_DEAD, x = 0;
-			if (i < en)
-			{
-				t = tri[i];
-				x = third[i];
-			}
-			const bool keep = !(t & INC_DEAD);
-			const uint32_t bal = __ballot_sync(FULL, keep);
-			if (keep)
-			{
-				const uint64_t o = out + __popc(bal & ((1u << lane) - 1u));
-				if (o < cap)
-				{
-					third2[o] = x;
-					tri2[o] = t;
-				}
-			}
-			out += __popc(bal);
-		}
-	}
-}
-
-// Copies the compacted lists (noff[m] entries, at most cap) and offsets back.
-__global__ void k_compact_back(const uint64_t *__restrict__ noff, uint64_t m, const uint32_t *__restrict__ third2,
-							   const uint32_t *__restrict__ tri2, uint64_t cap, uint64_t *__restrict__ off,
-							   uint32_t *__restrict__ third, uint32_t *__restrict__ tri)
-{
-	const uint64_t n = noff[m] < cap ? noff[m] : cap;
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n || i <= m; i += stride)
-	{
-		if (i < n)
-		{
-			third[i] = third2[i];
-			tri[i] = tri2[i];
-		}
-		if (i <= m)
-			off[i] = noff[i];
-	}
+	for (uint64_t e = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < m; e += stride)
+		span[e] = make_uint2(uint32_t(off[e]), uint32_t(off[e + 1]));
 }
 
 } // namespace
@@ -310,8 +236,10 @@ int build_incidence(Ctx &c, Incidence &inc)
 	const uint64_t T = c.T, m = c.m, n3 = 3 * T;
 	uint32_t *cnt = nullptr, *lists = nullptr, *counts = nullptr, *errf = nullptr;
 	unsigned long long *keys = nullptr, *scratch = nullptr, *maxlen = nullptr, *sumsq = nullptr;
+	uint64_t *off = nullptr;
 	int rc = NUCLEUS34_OK;
 	auto cleanup = [&] {
+		c.release(off);
 		c.release(cnt);
 		c.release(lists);
 		c.release(counts);
@@ -323,7 +251,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 	};
 	do
 	{
-		if ((rc = dalloc(c, &inc.off, m + 1, "incidence offsets")))
+		if ((rc = dalloc(c, &off, m + 1, "incidence offsets")))
 			break;
 		if ((rc = dalloc(c, &cnt, m, "incidence counts")))
 			break;
@@ -334,7 +262,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 		}
 		k_inc_count<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, cnt);
 		c.launches++;
-		if ((rc = scan_u32(c, cnt, inc.off, m)))
+		if ((rc = scan_u32(c, cnt, off, m)))
 			break;
 		if ((rc = dalloc(c, &keys, n3, "incidence keys")))
 			break;
@@ -350,7 +278,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 			rc = fail(NUCLEUS34_E_CUDA, "memset");
 			break;
 		}
-		k_inc_scatter<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, c.dsrc, c.dE, inc.off, cnt, keys, errf);
+		k_inc_scatter<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, c.dsrc, c.dE, off, cnt, keys, errf);
 		c.launches++;
 		c.release(cnt);
 		cnt = nullptr;
@@ -370,9 +298,9 @@ int build_incidence(Ctx &c, Incidence &inc)
 			rc = fail(NUCLEUS34_E_CUDA, "memset");
 			break;
 		}
-		k_seg_classify<<<grid_for(c, m, 256), 256, 0, c.stream>>>(inc.off, m, lists, counts, m, maxlen);
+		k_seg_classify<<<grid_for(c, m, 256), 256, 0, c.stream>>>(off, m, lists, counts, m, maxlen);
 		c.launches++;
-		k_sum_sq<<<grid_for(c, m, 256), 256, 0, c.stream>>>(inc.off, m, sumsq);
+		k_sum_sq<<<grid_for(c, m, 256), 256, 0, c.stream>>>(off, m, sumsq);
 		c.launches++;
 		uint32_t hcounts[4] = {0, 0, 0, 0};
 		unsigned long long hmax = 0;
@@ -393,7 +321,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 		}
 		if (hcounts[0])
 		{
-			k_seg_sort_warp<<<grid_for(c, hcounts[0], 8, 32), 256, 0, c.stream>>>(lists, counts + 0, inc.off, keys);
+			k_seg_sort_warp<<<grid_for(c, hcounts[0], 8, 32), 256, 0, c.stream>>>(lists, counts + 0, off, keys);
 			c.launches++;
 		}
 		if (hcounts[1])
@@ -401,7 +329,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 			const size_t smem = SEG_SMEM * sizeof(unsigned long long);
 			cudaFuncSetAttribute(k_seg_sort_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
 			k_seg_sort_block<<<grid_for(c, hcounts[1], 1, 2), SEG_BLOCK, smem, c.stream>>>(lists + m, counts + 1,
-																							inc.off, keys);
+																							off, keys);
 			c.launches++;
 		}
 		if (hcounts[2])
@@ -412,7 +340,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 			const uint32_t blocks = std::min<uint32_t>(hcounts[2], uint32_t(c.sm_count));
 			if ((rc = dalloc(c, &scratch, P * blocks, "segment sort scratch")))
 				break;
-			k_seg_sort_global<<<blocks, SEG_BLOCK, 0, c.stream>>>(lists + 2 * m, counts + 2, inc.off, keys,
+			k_seg_sort_global<<<blocks, SEG_BLOCK, 0, c.stream>>>(lists + 2 * m, counts + 2, off, keys,
 																  scratch, P);
 			c.launches++;
 		}
@@ -422,6 +350,10 @@ int build_incidence(Ctx &c, Incidence &inc)
 			break;
 		k_inc_split<<<grid_for(c, n3, 256), 256, 0, c.stream>>>(keys, n3, inc.third, inc.tri);
 		c.launches++;
+		if ((rc = dalloc(c, &inc.span, m ? m : 1, "incidence spans")))
+			break;
+		k_make_spans<<<grid_for(c, m, 256), 256, 0, c.stream>>>(off, m, inc.span);
+		c.launches++;
 		if (cudaGetLastError() != cudaSuccess)
 			rc = fail(NUCLEUS34_E_CUDA, "incidence kernels");
 	} while (false);
@@ -429,49 +361,9 @@ int build_incidence(Ctx &c, Incidence &inc)
 	return rc;
 }
 
-int compact_incidence(Ctx &c, Incidence &inc, uint64_t cap, uint32_t *err)
-{
-	const uint64_t m = c.m;
-	uint32_t *cnt = nullptr, *third2 = nullptr, *tri2 = nullptr;
-	uint64_t *noff = nullptr;
-	int rc = NUCLEUS34_OK;
-	do
-	{
-		if (cap > 3 * c.T)
-			cap = 3 * c.T;
-		if ((rc = dalloc(c, &cnt, m ? m : 1, "compaction counts")))
-			break;
-		if ((rc = dalloc(c, &noff, m + 1, "compaction offsets")))
-			break;
-		if ((rc = dalloc(c, &third2, cap ? cap : 1, "compaction third")))
-			break;
-		if ((rc = dalloc(c, &tri2, cap ? cap : 1, "compaction tri")))
-			break;
-		const uint32_t gw = grid_for(c, m, 256 / 32, 16);
-		k_alive_count<<<gw, 256, 0, c.stream>>>(inc.off, m, inc.tri, cnt);
-		c.launches++;
-		if ((rc = scan_u32(c, cnt, noff, m)))
-			break;
-		k_compact_copy<<<gw, 256, 0, c.stream>>>(inc.off, noff, m, inc.third, inc.tri, third2, tri2, cap, err);
-		c.launches++;
-		// Back into the same arrays (kernels captured with these pointers stay
-		// valid); the live count is read on the device, so nothing waits here.
-		k_compact_back<<<grid_for(c, cap > m + 1 ? cap : m + 1, 256), 256, 0, c.stream>>>(noff, m, third2, tri2, cap,
-																						   inc.off, inc.third, inc.tri);
-		c.launches++;
-		if (cudaGetLastError() != cudaSuccess)
-			rc = fail(NUCLEUS34_E_CUDA, "compaction kernels");
-	} while (false);
-	c.release(cnt);
-	c.release(noff);
-	c.release(third2);
-	c.release(tri2);
-	return rc;
-}
-
 void free_incidence(Ctx &c, Incidence &inc)
 {
-	c.release(inc.off);
+	c.release(inc.span);
 	c.release(inc.third);
 	c.release(inc.tri);
 	inc = Incidence{};

@@ -44,7 +44,11 @@ constexpr int PEEL_THREADS = 256;
 struct CtlX
 {
 	PeelCtl c;
-	uint32_t scan; // 1 while the next frontier must come from a scan
+	uint32_t scan;        // 1 while the next frontier must come from a scan
+	uint32_t compact_now; // set by k_compact_gate for the replay's compaction
+	unsigned long long peeled_at_compact;
+	unsigned long long live_at_compact;
+	uint32_t compactions;
 };
 
 __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
@@ -59,6 +63,10 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
 		z.level = 0xffffffffu; // "-1": the first level change tries level 0
 		ctl->c = z;
 		ctl->scan = 1;
+		ctl->compact_now = 0;
+		ctl->peeled_at_compact = 0;
+		ctl->live_at_compact = T;
+		ctl->compactions = 0;
 	}
 }
 
@@ -234,12 +242,12 @@ __device__ __forceinline__ void settle_clique(bool found, uint32_t t, uint32_t p
 }
 
 __device__ __forceinline__ Lists frontier_lists(uint32_t t, const uint32_t *__restrict__ tris,
-											   const uint64_t *__restrict__ incO)
+											   const uint2 *__restrict__ span)
 {
 	const uint32_t ea = __ldg(tris + 3 * uint64_t(t)), eb = __ldg(tris + 3 * uint64_t(t) + 1),
 				   ec = __ldg(tris + 3 * uint64_t(t) + 2);
-	return order_lists(uint32_t(incO[ea]), uint32_t(incO[ea + 1]), uint32_t(incO[eb]), uint32_t(incO[eb + 1]),
-					   uint32_t(incO[ec]), uint32_t(incO[ec + 1]));
+	const uint2 sa = __ldg(span + ea), sb = __ldg(span + eb), sc = __ldg(span + ec);
+	return order_lists(sa.x, sa.y, sb.x, sb.y, sc.x, sc.y);
 }
 
 // On-demand debit with the round-stamp owner test (used when triangle ids do
@@ -247,7 +255,7 @@ __device__ __forceinline__ Lists frontier_lists(uint32_t t, const uint32_t *__re
 // the longest list is found by a forward-moving binary search.
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_ondemand(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
-	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
+	const uint2 *__restrict__ span, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 	const int32_t *__restrict__ K, const uint32_t *__restrict__ R, int32_t *__restrict__ S, uint64_t T)
 {
 	if (ctl->c.done)
@@ -262,7 +270,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_ondemand(
 	for (uint64_t i = warp; i < nF; i += nwarps)
 	{
 		const uint32_t t = F[i];
-		const Lists L = frontier_lists(t, tris, incO);
+		const Lists L = frontier_lists(t, tris, span);
 		uint32_t lo_c = L.c0;
 		warp_intersect2<true>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
 												  uint32_t qb) {
@@ -385,21 +393,22 @@ constexpr uint32_t ID_MASK = 0x3fffffffu;
 // positions of triangle t's three entries: under b (third w), a (third v), c (third u)
 __device__ __forceinline__ void entry_positions(uint32_t t, const uint32_t *__restrict__ tris,
 												const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
-												const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third,
+												const uint2 *__restrict__ span, const uint32_t *__restrict__ third,
 												uint64_t pos[3])
 {
 	const uint32_t a = __ldg(tris + 3 * uint64_t(t)), b = __ldg(tris + 3 * uint64_t(t) + 1),
 				   c = __ldg(tris + 3 * uint64_t(t) + 2);
 	const uint32_t u = __ldg(src + b), v = __ldg(E + b), w = __ldg(E + c);
-	pos[0] = lower_bound32(third, uint32_t(incO[b]), uint32_t(incO[b + 1]), w);
-	pos[1] = lower_bound32(third, uint32_t(incO[a]), uint32_t(incO[a + 1]), v);
-	pos[2] = lower_bound32(third, uint32_t(incO[c]), uint32_t(incO[c + 1]), u);
+	const uint2 sa = __ldg(span + a), sb = __ldg(span + b), sc = __ldg(span + c);
+	pos[0] = lower_bound32(third, sb.x, sb.y, w);
+	pos[1] = lower_bound32(third, sa.x, sa.y, v);
+	pos[2] = lower_bound32(third, sc.x, sc.y, u);
 }
 
 __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
 							 int32_t *__restrict__ K, int32_t *__restrict__ S, const uint32_t *__restrict__ tris,
 							 const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
-							 const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third,
+							 const uint2 *__restrict__ span, const uint32_t *__restrict__ third,
 							 uint32_t *__restrict__ itri, uint64_t n3)
 {
 	if (ctl->c.done)
@@ -414,7 +423,7 @@ __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const u
 		K[t] = level;
 		S[t] = INT32_MAX;
 		uint64_t pos[3];
-		entry_positions(t, tris, src, E, incO, third, pos);
+		entry_positions(t, tris, src, E, span, third, pos);
 #pragma unroll
 		for (int r = 0; r < 3; ++r)
 			if (pos[r] < n3)
@@ -424,7 +433,7 @@ __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const u
 
 __global__ void k_finalize_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
 								 const uint32_t *__restrict__ tris, const uint32_t *__restrict__ src,
-								 const uint32_t *__restrict__ E, const uint64_t *__restrict__ incO,
+								 const uint32_t *__restrict__ E, const uint2 *__restrict__ span,
 								 const uint32_t *__restrict__ third, uint32_t *__restrict__ itri, uint64_t n3)
 {
 	if (ctl->c.done)
@@ -436,7 +445,7 @@ __global__ void k_finalize_flags(CtlX *ctl, const uint32_t *__restrict__ F0, con
 	{
 		const uint32_t t = F[i];
 		uint64_t pos[3];
-		entry_positions(t, tris, src, E, incO, third, pos);
+		entry_positions(t, tris, src, E, span, third, pos);
 #pragma unroll
 		for (int r = 0; r < 3; ++r)
 			if (pos[r] < n3)
@@ -469,7 +478,7 @@ __device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q
 // therefore means the clique was destroyed before.
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
-	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
+	const uint2 *__restrict__ span, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 	int32_t *__restrict__ S, uint64_t T)
 {
 	if (ctl->c.done)
@@ -484,7 +493,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	for (uint64_t fi = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; fi < nF; fi += stride)
 	{
 		const uint32_t t = F[fi];
-		const Lists L = frontier_lists(t, tris, incO);
+		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 > THREAD_MODE_MAX)
 			continue; // the warp kernel takes it
 		uint32_t lo_b = L.b0, lo_c = L.c0;
@@ -530,7 +539,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 // longest list only when its two other partners are still alive.
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
-	const uint64_t *__restrict__ incO, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
+	const uint2 *__restrict__ span, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 	int32_t *__restrict__ S, uint64_t T)
 {
 	if (ctl->c.done)
@@ -546,7 +555,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 	for (uint64_t fi = warp; fi < nF; fi += nwarps)
 	{
 		const uint32_t t = F[fi];
-		const Lists L = frontier_lists(t, tris, incO);
+		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 <= THREAD_MODE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
 		uint32_t lo_c = L.c0;
@@ -587,6 +596,67 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 				}
 			}
 		});
+	}
+}
+
+// Compaction gate, run after each replay: once the triangles peeled since
+// the last compaction reach 1/N34_COMPACT_DIV of the live ones then, the next
+// k_compact_spans drops the dead entries. A compaction reads every remaining
+// entry once, so the passes form a geometric series (at most N34_COMPACT_DIV
+// passes over the full incidence in total).
+__global__ void k_compact_gate(CtlX *ctl, uint64_t T)
+{
+	const unsigned long long peeled = ctl->c.peeled;
+	ctl->compact_now = 0;
+	if (ctl->c.done || peeled >= T)
+		return;
+	if (N34_COMPACT_DIV * (peeled - ctl->peeled_at_compact) >= ctl->live_at_compact)
+	{
+		ctl->compact_now = 1;
+		ctl->peeled_at_compact = peeled;
+		ctl->live_at_compact = T - peeled;
+		ctl->compactions++;
+	}
+}
+
+// In-place compaction of every edge list (one warp per edge): live entries
+// move to the front of the list, keeping their order, and the span's end is
+// lowered. A tile is fully read (warp ballot) before any lane writes, and the
+// write cursor never passes the tile's start, so unread entries stay intact.
+__global__ void __launch_bounds__(PEEL_THREADS) k_compact_spans(const CtlX *ctl, uint2 *__restrict__ span,
+																  uint64_t m, uint32_t *__restrict__ third,
+																  uint32_t *__restrict__ itri)
+{
+	if (!ctl->compact_now)
+		return;
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	const uint32_t lane = lane_id();
+	for (uint64_t e = warp; e < m; e += nwarps)
+	{
+		const uint2 sp = span[e];
+		uint32_t out = sp.x;
+		for (uint32_t base = sp.x; base < sp.y; base += 32)
+		{
+			const uint32_t i = base + lane;
+			uint32_t t = DEAD, x = 0;
+			if (i < sp.y)
+			{
+				t = itri[i];
+				x = third[i];
+			}
+			const bool keep = !(t & DEAD);
+			const uint32_t bal = __ballot_sync(FULL, keep);
+			const uint32_t o = out + __popc(bal & lanemask_lt());
+			if (keep && o != i)
+			{
+				third[o] = x;
+				itri[o] = t;
+			}
+			out += __popc(bal);
+		}
+		if (lane == 0 && out != sp.y)
+			span[e].y = out;
 	}
 }
 
@@ -709,16 +779,16 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				cudaMemcpyAsync(trace, &ctl->c, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream);
 			if (flags)
 			{
-				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.off,
+				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.span,
 																   inc.third, inc.tri, 3 * T);
 				tick(4);
-				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off,
+				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.span,
 																		   inc.third, inc.tri, S, T);
 				tick(5);
-				k_debit_flags_warp<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off, inc.third,
+				k_debit_flags_warp<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.span, inc.third,
 																		 inc.tri, S, T);
 				tick(6);
-				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, c.dsrc, c.dE, inc.off,
+				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, c.dsrc, c.dE, inc.span,
 																	   inc.third, inc.tri, 3 * T);
 				tick(7);
 			}
@@ -727,7 +797,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				k_mark<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, R, S);
 				tick(4);
 				if (variant == NUCLEUS34_ONDEMAND)
-					k_debit_ondemand<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.off, inc.third,
+					k_debit_ondemand<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.span, inc.third,
 																		   inc.tri, K, R, S, T);
 				else
 					k_debit_direct<<<gwarp, PEEL_THREADS, 0, c.stream>>>(
@@ -749,10 +819,20 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		cudaGraph_t graph = nullptr;
 		cudaGraphExec_t exec = nullptr;
 		bool use_graph = !profile && cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+		const uint32_t gcompact = grid_for(c, c.m, PEEL_THREADS / 32, 16);
+		// after every ROUNDS_PER_GRAPH rounds: the gated in-place compaction
+		auto launch_compaction = [&]() {
+			if (!flags)
+				return;
+			k_compact_gate<<<1, 1, 0, c.stream>>>(ctl, T);
+			k_compact_spans<<<gcompact, PEEL_THREADS, 0, c.stream>>>(ctl, inc.span, c.m, inc.third, inc.tri);
+		};
+		const uint32_t per_replay = flags ? 2u : 0u;
 		if (use_graph)
 		{
 			for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
 				launch_round(nullptr, nullptr);
+			launch_compaction();
 			use_graph = cudaStreamEndCapture(c.stream, &graph) == cudaSuccess && graph &&
 						cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
 		}
@@ -771,14 +851,6 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			for (auto &e : events)
 				cudaEventCreate(&e);
 		}
-		// Compaction of the incidence (death-flag peel only): once the
-		// triangles peeled since the last compaction reach 1/N34_COMPACT_DIV
-		// of the live ones then, the dead entries are dropped so that later
-		// rounds scan shorter lists. A compaction costs one pass over the live
-		// entries, so the passes form a geometric series (at most
-		// N34_COMPACT_DIV passes over the full incidence in total).
-		uint64_t live_at_compact = T, peeled_at_compact = 0, compactions = 0;
-		bool compaction_on = flags;
 		// Bounded host loop: every round that is not a no-op peels at least one
 		// triangle, so T + 1 rounds suffice; the bound leaves a wide margin.
 		// The next replay is queued before the host reads the control block of
@@ -799,11 +871,14 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 					return false;
 			}
 			else
+			{
 				for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
 					launch_round(profile ? &events[size_t(r) * (PROF_STEPS + 1)] : nullptr,
 								 trace_buf ? trace_buf + 3 * r : nullptr);
+				launch_compaction();
+			}
 			rounds += ROUNDS_PER_GRAPH;
-			c.launches += uint64_t(ROUNDS_PER_GRAPH) * per_round;
+			c.launches += uint64_t(ROUNDS_PER_GRAPH) * per_round + per_replay;
 			return cudaMemcpyAsync(&ring[slot], &ctl->c, sizeof(PeelCtl), cudaMemcpyDeviceToHost, c.stream) ==
 					   cudaSuccess &&
 				   cudaEventRecord(ring_ev[slot], c.stream) == cudaSuccess;
@@ -857,32 +932,6 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				rc = fail(NUCLEUS34_E_TIMEOUT, "peel did not converge within its round bound");
 				break;
 			}
-			if (compaction_on && hc.peeled < T &&
-				N34_COMPACT_DIV * (hc.peeled - peeled_at_compact) >= live_at_compact)
-			{
-				// queued behind the replay in flight, when no fewer triangles are
-				// peeled: 3 entries per live triangle bound the live entries
-				Incidence view = inc; // same arrays; only their contents change
-				const int crc = compact_incidence(c, view, 3 * (T - hc.peeled), &ctl->c.error);
-				if (crc == NUCLEUS34_E_OOM_BUDGET)
-				{
-					// no room for the temporaries: keep peeling on the full lists
-					compaction_on = false;
-					cudaGetLastError();
-					clear_error();
-				}
-				else if (crc)
-				{
-					rc = crc;
-					break;
-				}
-				else
-				{
-					live_at_compact = T - hc.peeled;
-					peeled_at_compact = hc.peeled;
-					compactions++;
-				}
-			}
 			if (!enqueue(int(issued & 1)))
 			{
 				rc = fail(NUCLEUS34_E_CUDA, "peel replay launch");
@@ -904,8 +953,9 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			cudaFreeHost(trace_buf);
 		if (profile)
 		{
-			std::fprintf(stderr, "[peel-profile] rounds=%llu compactions=%llu", (unsigned long long)rounds,
-						 (unsigned long long)compactions);
+			uint32_t compactions = 0;
+			cudaMemcpy(&compactions, &ctl->compactions, 4, cudaMemcpyDeviceToHost);
+			std::fprintf(stderr, "[peel-profile] rounds=%llu compactions=%u", (unsigned long long)rounds, compactions);
 			for (int j = 0; j < PROF_STEPS; ++j)
 				std::fprintf(stderr, " %s=%.1fms", prof_names[j], prof_ms[j]);
 			std::fprintf(stderr, "\n");

@@ -5,10 +5,13 @@
 
 namespace n34 {
 
-// Edge -> triangle incidence, per edge sorted by third vertex.
+// Edge -> triangle incidence, per edge sorted by third vertex. Edge e's list
+// is [span[e].x, span[e].y) in third[] / tri[] (32-bit positions: the
+// incidence holds 3T < 2^32 entries). The peel may shorten a list in place
+// (dead entries dropped, span[e].y lowered); begins never move.
 struct Incidence
 {
-	uint64_t *off = nullptr;   // m+1
+	uint2 *span = nullptr;     // m
 	uint32_t *third = nullptr; // 3T
 	uint32_t *tri = nullptr;   // 3T
 	unsigned long long sum_te_sq = 0; // sum over edges of (list length)^2
@@ -34,11 +37,6 @@ cudaError_t launch_tri_write(const uint32_t *O, const uint32_t *E, uint64_t n, c
 int list_triangles(Ctx &c);
 int build_incidence(Ctx &c, Incidence &inc);
 void free_incidence(Ctx &c, Incidence &inc);
-// Drops the entries marked INC_DEAD from every edge list, in place (same
-// arrays, shorter segments, order kept), stream-ordered and without waiting
-// on the host. cap bounds the live entries (3 per live triangle); a larger
-// count sets bit 2 in *err and the copy stops at cap.
-int compact_incidence(Ctx &c, Incidence &inc, uint64_t cap, uint32_t *err);
 // support[t] = number of four-cliques on t; returns sum(support) in *total.
 // own (optional): cliques whose lowest triangle is t (direct variant sizes).
 int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total, uint32_t *own);

@@ -29,24 +29,18 @@ struct TriEdges
 	uint32_t b0, e0, b1, e1, b2, e2;
 };
 
-__device__ __forceinline__ TriEdges tri_lists(const uint32_t *__restrict__ tris, const uint64_t *__restrict__ incO,
+__device__ __forceinline__ TriEdges tri_lists(const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
 											  uint64_t t)
 {
 	const uint32_t a = __ldg(tris + 3 * t + 0), b = __ldg(tris + 3 * t + 1), c = __ldg(tris + 3 * t + 2);
-	TriEdges L;
-	L.b0 = uint32_t(incO[a]);
-	L.e0 = uint32_t(incO[a + 1]);
-	L.b1 = uint32_t(incO[b]);
-	L.e1 = uint32_t(incO[b + 1]);
-	L.b2 = uint32_t(incO[c]);
-	L.e2 = uint32_t(incO[c + 1]);
-	return L;
+	const uint2 sa = __ldg(span + a), sb = __ldg(span + b), sc = __ldg(span + c);
+	return TriEdges{sa.x, sa.y, sb.x, sb.y, sc.x, sc.y};
 }
 
-__device__ __forceinline__ Lists tri_order(const uint32_t *__restrict__ tris, const uint64_t *__restrict__ incO,
+__device__ __forceinline__ Lists tri_order(const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
 										   uint64_t t)
 {
-	const TriEdges E = tri_lists(tris, incO, t);
+	const TriEdges E = tri_lists(tris, span, t);
 	return order_lists(E.b0, E.e0, E.b1, E.e1, E.b2, E.e2);
 }
 
@@ -59,7 +53,7 @@ __device__ __forceinline__ Lists tri_order(const uint32_t *__restrict__ tris, co
 // by a forward-moving binary search.
 template <bool WITH_OWN>
 __global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__restrict__ tris, uint64_t T,
-															const uint64_t *__restrict__ incO,
+															const uint2 *__restrict__ span,
 															const uint32_t *__restrict__ third,
 															const uint32_t *__restrict__ itri,
 															int32_t *__restrict__ support, uint32_t *__restrict__ own,
@@ -75,7 +69,7 @@ __global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__re
 		const bool valid = t < T;
 		Lists L{};
 		if (valid)
-			L = tri_order(tris, incO, t);
+			L = tri_order(tris, span, t);
 		const bool small = valid && L.a1 - L.a0 <= THREAD_MODE_MAX;
 		if (small)
 		{
@@ -161,7 +155,7 @@ __device__ __forceinline__ void sort3(uint32_t &a, uint32_t &b, uint32_t &c)
 // Writes each triangle's owned cliques (lowest member t) at qoff[t], in
 // ascending fourth-vertex order; same hybrid thread/warp split as k_support.
 __global__ void __launch_bounds__(SUP_THREADS, 4) k_clique_write(const uint32_t *__restrict__ tris, uint64_t T,
-																 const uint64_t *__restrict__ incO,
+																 const uint2 *__restrict__ span,
 																 const uint32_t *__restrict__ third,
 																 const uint32_t *__restrict__ itri,
 																 const uint64_t *__restrict__ qoff,
@@ -182,7 +176,7 @@ __global__ void __launch_bounds__(SUP_THREADS, 4) k_clique_write(const uint32_t 
 			out_end = qoff[t + 1];
 			work = out < out_end;
 			if (work)
-				L = tri_order(tris, incO, t);
+				L = tri_order(tris, span, t);
 		}
 		const bool small = work && L.a1 - L.a0 <= THREAD_MODE_MAX;
 		if (small)
@@ -275,10 +269,10 @@ int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *tota
 		}
 		const uint32_t grid = grid_for(c, (c.T + 31) / 32, SUP_THREADS / 32, 32);
 		if (own)
-			k_support<true><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.off, inc.third, inc.tri, support,
+			k_support<true><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.span, inc.third, inc.tri, support,
 																own, dtot);
 		else
-			k_support<false><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.off, inc.third, inc.tri,
+			k_support<false><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.span, inc.third, inc.tri,
 																 support, nullptr, dtot);
 		c.launches++;
 		unsigned long long h = 0;
@@ -332,7 +326,7 @@ int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, const uin
 			break;
 		if ((rc = dalloc(c, &c.dquds, 4 * Q, "four-cliques")))
 			break;
-		k_clique_write<<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, T, inc.off, inc.third, inc.tri, qoff,
+		k_clique_write<<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, T, inc.span, inc.third, inc.tri, qoff,
 														   reinterpret_cast<uint4 *>(c.dquds));
 		c.launches++;
 		c.release(qoff);
