@@ -243,7 +243,11 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 		}
 		if (c.T)
 		{
-			if ((rc = build_incidence(c, inc)))
+			// the on-demand peel with death flags (T < 2^30) keeps each
+			// triangle's entry positions
+			const bool want_tpos =
+				variant == NUCLEUS34_ONDEMAND && c.T <= 0x3fffffffull && !(c.opt_flags & NUCLEUS34_OPT_STAMP_PEEL);
+			if ((rc = build_incidence(c, inc, want_tpos)))
 				break;
 			r.sum_te_sq = inc.sum_te_sq;
 		}

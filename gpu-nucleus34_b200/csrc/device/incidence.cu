@@ -38,7 +38,7 @@ __global__ void k_inc_count(const uint32_t *__restrict__ tris, uint64_t T, uint3
 __global__ void k_inc_scatter(const uint32_t *__restrict__ tris, uint64_t T, const uint32_t *__restrict__ src,
 							  const uint32_t *__restrict__ E, const uint64_t *__restrict__ incO,
 							  uint32_t *__restrict__ cursor, unsigned long long *__restrict__ keys,
-							  uint32_t *__restrict__ err)
+							  uint32_t *__restrict__ err, bool slot_bits)
 {
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
@@ -54,7 +54,7 @@ __global__ void k_inc_scatter(const uint32_t *__restrict__ tris, uint64_t T, con
 			const uint32_t s = atomicAdd(cursor + e, 1u);
 			// capacity guard: the counts pass sized every segment exactly
 			if (incO[e] + s < incO[e + 1])
-				keys[incO[e] + s] = (uint64_t(x3[r]) << 32) | t;
+				keys[incO[e] + s] = (uint64_t(x3[r]) << 32) | (slot_bits ? (t | (uint64_t(r) << 30)) : t);
 			else
 				atomicOr(err, 1u);
 		}
@@ -209,15 +209,25 @@ __global__ void k_sum_sq(const uint64_t *__restrict__ off, uint64_t m, unsigned 
 		atomicAdd(out, acc);
 }
 
+// Splits the sorted keys into third[] and tri[]; with tpos, the key's slot
+// bits (30-31: which of the triangle's three entries) give tpos[3t + slot].
 __global__ void k_inc_split(const unsigned long long *__restrict__ keys, uint64_t n, uint32_t *__restrict__ third,
-							uint32_t *__restrict__ tri)
+							uint32_t *__restrict__ tri, uint32_t *__restrict__ tpos)
 {
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
 	{
 		const unsigned long long k = keys[i];
 		third[i] = uint32_t(k >> 32);
-		tri[i] = uint32_t(k);
+		const uint32_t lo = uint32_t(k);
+		if (tpos)
+		{
+			const uint32_t t = lo & 0x3fffffffu;
+			tri[i] = t;
+			tpos[3 * uint64_t(t) + (lo >> 30)] = uint32_t(i);
+		}
+		else
+			tri[i] = lo;
 	}
 }
 
@@ -231,7 +241,7 @@ __global__ void k_make_spans(const uint64_t *__restrict__ off, uint64_t m, uint2
 
 } // namespace
 
-int build_incidence(Ctx &c, Incidence &inc)
+int build_incidence(Ctx &c, Incidence &inc, bool want_tpos)
 {
 	const uint64_t T = c.T, m = c.m, n3 = 3 * T;
 	uint32_t *cnt = nullptr, *lists = nullptr, *counts = nullptr, *errf = nullptr;
@@ -278,7 +288,18 @@ int build_incidence(Ctx &c, Incidence &inc)
 			rc = fail(NUCLEUS34_E_CUDA, "memset");
 			break;
 		}
-		k_inc_scatter<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, c.dsrc, c.dE, off, cnt, keys, errf);
+		// entry positions per triangle (the on-demand peel's death flags);
+		// optional: without room for them the peel searches instead
+		if (want_tpos && T <= 0x3fffffffull)
+		{
+			if (dalloc(c, &inc.tpos, 3 * T, "triangle entry positions"))
+			{
+				inc.tpos = nullptr;
+				clear_error();
+			}
+		}
+		k_inc_scatter<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, c.dsrc, c.dE, off, cnt, keys, errf,
+																 inc.tpos != nullptr);
 		c.launches++;
 		c.release(cnt);
 		cnt = nullptr;
@@ -348,7 +369,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 			break;
 		if ((rc = dalloc(c, &inc.tri, n3, "incidence tri")))
 			break;
-		k_inc_split<<<grid_for(c, n3, 256), 256, 0, c.stream>>>(keys, n3, inc.third, inc.tri);
+		k_inc_split<<<grid_for(c, n3, 256), 256, 0, c.stream>>>(keys, n3, inc.third, inc.tri, inc.tpos);
 		c.launches++;
 		if ((rc = dalloc(c, &inc.span, m ? m : 1, "incidence spans")))
 			break;
@@ -364,6 +385,7 @@ int build_incidence(Ctx &c, Incidence &inc)
 void free_incidence(Ctx &c, Incidence &inc)
 {
 	c.release(inc.span);
+	c.release(inc.tpos);
 	c.release(inc.third);
 	c.release(inc.tri);
 	inc = Incidence{};

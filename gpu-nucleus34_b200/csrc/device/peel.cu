@@ -390,12 +390,20 @@ constexpr uint32_t DEAD = INC_DEAD;
 constexpr uint32_t DYING = 0x40000000u;
 constexpr uint32_t ID_MASK = 0x3fffffffu;
 
-// positions of triangle t's three entries: under b (third w), a (third v), c (third u)
+// positions of triangle t's three entries: under b (third w), a (third v), c (third u);
+// read from tpos when the incidence keeps them, else searched
 __device__ __forceinline__ void entry_positions(uint32_t t, const uint32_t *__restrict__ tris,
 												const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
 												const uint2 *__restrict__ span, const uint32_t *__restrict__ third,
-												uint64_t pos[3])
+												const uint32_t *__restrict__ tpos, uint64_t pos[3])
 {
+	if (tpos)
+	{
+		pos[0] = tpos[3 * uint64_t(t)];
+		pos[1] = tpos[3 * uint64_t(t) + 1];
+		pos[2] = tpos[3 * uint64_t(t) + 2];
+		return;
+	}
 	const uint32_t a = __ldg(tris + 3 * uint64_t(t)), b = __ldg(tris + 3 * uint64_t(t) + 1),
 				   c = __ldg(tris + 3 * uint64_t(t) + 2);
 	const uint32_t u = __ldg(src + b), v = __ldg(E + b), w = __ldg(E + c);
@@ -409,7 +417,7 @@ __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const u
 							 int32_t *__restrict__ K, int32_t *__restrict__ S, const uint32_t *__restrict__ tris,
 							 const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
 							 const uint2 *__restrict__ span, const uint32_t *__restrict__ third,
-							 uint32_t *__restrict__ itri, uint64_t n3)
+							 const uint32_t *__restrict__ tpos, uint32_t *__restrict__ itri, uint64_t n3)
 {
 	if (ctl->c.done)
 		return;
@@ -423,7 +431,7 @@ __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const u
 		K[t] = level;
 		S[t] = INT32_MAX;
 		uint64_t pos[3];
-		entry_positions(t, tris, src, E, span, third, pos);
+		entry_positions(t, tris, src, E, span, third, tpos, pos);
 #pragma unroll
 		for (int r = 0; r < 3; ++r)
 			if (pos[r] < n3)
@@ -434,7 +442,8 @@ __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const u
 __global__ void k_finalize_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
 								 const uint32_t *__restrict__ tris, const uint32_t *__restrict__ src,
 								 const uint32_t *__restrict__ E, const uint2 *__restrict__ span,
-								 const uint32_t *__restrict__ third, uint32_t *__restrict__ itri, uint64_t n3)
+								 const uint32_t *__restrict__ third, const uint32_t *__restrict__ tpos,
+								 uint32_t *__restrict__ itri, uint64_t n3)
 {
 	if (ctl->c.done)
 		return;
@@ -445,7 +454,7 @@ __global__ void k_finalize_flags(CtlX *ctl, const uint32_t *__restrict__ F0, con
 	{
 		const uint32_t t = F[i];
 		uint64_t pos[3];
-		entry_positions(t, tris, src, E, span, third, pos);
+		entry_positions(t, tris, src, E, span, third, tpos, pos);
 #pragma unroll
 		for (int r = 0; r < 3; ++r)
 			if (pos[r] < n3)
@@ -535,13 +544,21 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 }
 
 // Debit of dying triangles with long lists: one warp each, tile merge (or
-// binary search) of the two shortest lists; a found x is looked up in the
-// longest list only when its two other partners are still alive.
-__global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
+// binary search) of the two shortest lists. A common third whose two
+// partners on A and B are alive is queued in shared memory; the queue is
+// resolved 32 entries at a time (each lane one lookup on the longest list),
+// so the dependent search chain is paid once per 32 live cliques instead of
+// once per merge step that has any.
+#ifndef N34_DEBIT_MINB
+#define N34_DEBIT_MINB 8
+#endif
+__global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
 	const uint2 *__restrict__ span, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 	int32_t *__restrict__ S, uint64_t T)
 {
+	constexpr int WARPS = PEEL_THREADS / 32;
+	__shared__ uint32_t qx[WARPS][64], qp0[WARPS][64], qp1[WARPS][64];
 	if (ctl->c.done)
 		return;
 	const uint32_t nF = ctl->c.nF;
@@ -550,6 +567,8 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 	const int32_t level = int32_t(ctl->c.level);
 	uint32_t *nNext = &ctl->c.nNext;
 	uint32_t *err = &ctl->c.error;
+	const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+	uint32_t *bx = qx[wib], *b0 = qp0[wib], *b1 = qp1[wib];
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
 	for (uint64_t fi = warp; fi < nF; fi += nwarps)
@@ -559,24 +578,19 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 		if (L.a1 - L.a0 <= THREAD_MODE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
 		uint32_t lo_c = L.c0;
-		warp_intersect2<true>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
-												  uint32_t qb) {
-			uint32_t q0 = DEAD, q1 = DEAD, q2 = DEAD;
-			bool live = false;
-			if (found)
-			{
-				q0 = qa;
-				q1 = qb;
-				live = !(q0 & DEAD) && !(q1 & DEAD);
-			}
-			const uint32_t fm = __ballot_sync(FULL, live);
-			if (!fm)
-				return;
-			const uint32_t pc = warp_lower_bound(third, lo_c, L.c1, live, x);
-			lo_c = __shfl_sync(FULL, pc, 31 - __clz(fm));
+		uint32_t queued = 0; // warp-uniform
+		// resolves the first n (<= 32) queued entries; called by all lanes
+		auto resolve = [&](uint32_t n) {
+			__syncwarp();
+			const bool v = lane < n;
+			const uint32_t x = v ? bx[lane] : 0xffffffffu;
+			const uint32_t q0 = v ? b0[lane] : DEAD, q1 = v ? b1[lane] : DEAD;
+			const uint32_t pc = warp_lower_bound(third, lo_c, L.c1, v, x);
+			lo_c = __shfl_sync(FULL, pc, n - 1); // thirds ascend through the queue
 			bool hit[3] = {false, false, false};
+			uint32_t q2 = DEAD;
 			// absent from C: that partner died and was compacted away (clique destroyed)
-			if (live && pc < L.c1 && __ldg(third + pc) == x)
+			if (v && pc < L.c1 && __ldg(third + pc) == x)
 			{
 				q2 = __ldg(itri + pc);
 				if (!(q2 & DEAD))
@@ -595,7 +609,47 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_warp(
 						atomicOr(err, 1u);
 				}
 			}
+			__syncwarp();
+		};
+		warp_intersect2<true>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
+												  uint32_t qb) {
+			const bool live = found && !(qa & DEAD) && !(qb & DEAD);
+			const uint32_t fm = __ballot_sync(FULL, live);
+			if (!fm)
+				return;
+			const uint32_t o = queued + __popc(fm & lanemask_lt());
+			if (live)
+			{
+				bx[o] = x;
+				b0[o] = qa;
+				b1[o] = qb;
+			}
+			queued += __popc(fm);
+			if (queued >= 32)
+			{
+				resolve(32);
+				// move the overflow [32, queued) to the front (ranges do not overlap)
+				const uint32_t rest = queued - 32;
+				uint32_t mx = 0, m0 = 0, m1 = 0;
+				if (lane < rest)
+				{
+					mx = bx[32 + lane];
+					m0 = b0[32 + lane];
+					m1 = b1[32 + lane];
+				}
+				__syncwarp();
+				if (lane < rest)
+				{
+					bx[lane] = mx;
+					b0[lane] = m0;
+					b1[lane] = m1;
+				}
+				queued = rest;
+			}
 		});
+		if (queued)
+			resolve(queued);
+		__syncwarp();
 	}
 }
 
@@ -625,7 +679,7 @@ __global__ void k_compact_gate(CtlX *ctl, uint64_t T)
 // write cursor never passes the tile's start, so unread entries stay intact.
 __global__ void __launch_bounds__(PEEL_THREADS) k_compact_spans(const CtlX *ctl, uint2 *__restrict__ span,
 																  uint64_t m, uint32_t *__restrict__ third,
-																  uint32_t *__restrict__ itri)
+																  uint32_t *__restrict__ itri, uint32_t *__restrict__ tpos)
 {
 	if (!ctl->compact_now)
 		return;
@@ -652,6 +706,13 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_compact_spans(const CtlX *ctl,
 			{
 				third[o] = x;
 				itri[o] = t;
+				if (tpos)
+				{
+					// the moved entry is the one of t's three recorded at i
+					uint32_t *tp = tpos + 3 * uint64_t(t);
+					const uint32_t r = tp[0] == i ? 0u : (tp[1] == i ? 1u : 2u);
+					tp[r] = o;
+				}
 			}
 			out += __popc(bal);
 		}
@@ -780,7 +841,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			if (flags)
 			{
 				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.span,
-																   inc.third, inc.tri, 3 * T);
+																   inc.third, inc.tpos, inc.tri, 3 * T);
 				tick(4);
 				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.span,
 																		   inc.third, inc.tri, S, T);
@@ -789,7 +850,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 																		 inc.tri, S, T);
 				tick(6);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, c.dsrc, c.dE, inc.span,
-																	   inc.third, inc.tri, 3 * T);
+																	   inc.third, inc.tpos, inc.tri, 3 * T);
 				tick(7);
 			}
 			else
@@ -825,7 +886,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			if (!flags)
 				return;
 			k_compact_gate<<<1, 1, 0, c.stream>>>(ctl, T);
-			k_compact_spans<<<gcompact, PEEL_THREADS, 0, c.stream>>>(ctl, inc.span, c.m, inc.third, inc.tri);
+			k_compact_spans<<<gcompact, PEEL_THREADS, 0, c.stream>>>(ctl, inc.span, c.m, inc.third, inc.tri,
+																	  inc.tpos);
 		};
 		const uint32_t per_replay = flags ? 2u : 0u;
 		if (use_graph)

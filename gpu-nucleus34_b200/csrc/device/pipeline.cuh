@@ -14,6 +14,9 @@ struct Incidence
 	uint2 *span = nullptr;     // m
 	uint32_t *third = nullptr; // 3T
 	uint32_t *tri = nullptr;   // 3T
+	// optional (on-demand peel with death flags): tpos[3t + r] = position of
+	// triangle t's entry under its edge b (r=0), a (r=1), c (r=2)
+	uint32_t *tpos = nullptr;
 	unsigned long long sum_te_sq = 0; // sum over edges of (list length)^2
 };
 
@@ -35,7 +38,7 @@ cudaError_t launch_tri_count(const uint32_t *O, const uint32_t *E, uint64_t n, u
 cudaError_t launch_tri_write(const uint32_t *O, const uint32_t *E, uint64_t n, const uint64_t *toff,
 							 uint32_t *tris, int sm_count, cudaStream_t s);
 int list_triangles(Ctx &c);
-int build_incidence(Ctx &c, Incidence &inc);
+int build_incidence(Ctx &c, Incidence &inc, bool want_tpos);
 void free_incidence(Ctx &c, Incidence &inc);
 // support[t] = number of four-cliques on t; returns sum(support) in *total.
 // own (optional): cliques whose lowest triangle is t (direct variant sizes).
