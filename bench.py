@@ -242,6 +242,12 @@ def main():
     launches = sum(r["gpu_launches"] for r in results)
     ctx.close()
 
+    # ---- one untimed run with per-kernel CUDA events in the peel: device time
+    # of the re-enumeration (debit) kernels for the roofline ----
+    with n34.Context(device=device, flags=n34.OPT_PROFILE_PEEL) as pctx:
+        pctx.upload(g)
+        prof = pctx.run(a.variant)
+
     # ---- end-to-end through the one-shot C-ABI call (e2e) ----
     e2e = None
     if not a.no_e2e:
@@ -311,7 +317,7 @@ def main():
     }
     if e2e:
         line["e2e"] = e2e
-    line["roofline"], line["roofline_support"] = roofline(r, peaks, peak_kind)
+    line["roofline"], line["roofline_support"] = roofline(r, prof, peaks, peak_kind)
     if not a.no_cpu_baseline:
         try:
             cb = cpu_reference_run(a, 1)
@@ -322,36 +328,45 @@ def main():
     return 0
 
 
-# DRAM bytes per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-# on a smaller case of the same workload and scaled by the algorithmic bytes;
-# filled from profiles/  -- None until captured.
-NCU_TRAFFIC_PER_ALG_BYTE = {"k_support": None, "k_debit_ondemand": None}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
+# byte, from ncu captures of a smaller case of the same workload (R-MAT scale
+# 17; profiles/), applied to this run's algorithmic bytes: the traffic of both
+# kernels grows with the lists they read.
+NCU_TRAFFIC_PER_ALG_BYTE = {"debit": None, "k_support": None}
 
 
-def roofline(r, peaks, kind):
-    """HBM roofline of the two intersection kernels.
+def roofline(r, prof, peaks, kind):
+    """HBM roofline of the two intersection phases.
 
-    Algorithmic bytes of one full enumeration (the 3-way intersections of all
-    triangles) use the zipper bound 4*sum_e T(e)^2 + 36*T + 48*Q: each triangle
-    reads its three edges' incidence lists (4 B per entry), its own record and
-    list bounds (36 B), and each of the 4Q clique occurrences reads 3 partner
-    ids (48 B per clique). The support count performs one enumeration in one
-    launch; the peel performs it once more, spread over its rounds."""
+    Algorithmic bytes of one full enumeration (every triangle's lists
+    intersected once) use the zipper bound 4*sum_e T(e)^2 + 36*T + 48*Q: each
+    triangle reads its three edges' incidence lists (4 B per entry), its own
+    record and list bounds (36 B), and each of the 4Q clique occurrences reads
+    3 partner ids (48 B per clique). The support count performs one
+    enumeration in one launch (k_support); the peel performs it once more,
+    spread over its rounds (k_debit_flags_warp + k_debit_flags_thread, two
+    launches per round), timed by CUDA events around those kernels in a
+    separate profiling run of the same workload. Both kernels intersect only
+    the two shortest lists of a triangle, so they move fewer bytes than this
+    bound and a fraction above 1 is possible."""
     T, Q, S2 = r["triangle_count"], r["four_clique_count"], r["sum_te_sq"]
     alg = 4 * S2 + 36 * T + 48 * Q
     peak = peaks.get("hbm_gbs")
+    pk = f"{kind} ({'hbm_gbs' if kind == 'measured' else 'fallback 6.65 TB/s'})"
     out = []
-    for name, t, what in (("k_debit_ondemand", r["t_peel"], "peel re-enumeration (all rounds)"),
-                          ("k_support", r["t_support"], "support count (one launch)")):
+    for name, key, t, launches, what in (
+            ("k_debit_flags_warp+k_debit_flags_thread", "debit", prof.get("t_peel_debit", 0.0),
+             2 * int(prof.get("peeling_iterations", 0)), "peel re-enumeration, all rounds (profiling run)"),
+            ("k_support", "k_support", r["t_support"], 1, "support count (one launch, timed run)")):
         ach = alg / t / 1e9 if t > 0 else None
-        ratio = NCU_TRAFFIC_PER_ALG_BYTE.get(name)
+        ratio = NCU_TRAFFIC_PER_ALG_BYTE.get(key)
         out.append({"kernel": name, "what": what, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                     "frac": (ach / peak) if (ach and peak) else None,
                     "traffic": (ratio * alg) if ratio else None, "algorithmic_bytes": alg,
-                    "peak_kind": f"{kind} ({'hbm_gbs' if kind == 'measured' else 'fallback 6.65 TB/s'})",
-                    "definition": "4*sum_e T(e)^2 + 36T + 48Q bytes per full enumeration"})
-    # the dominant kernel is the one with the larger phase time
-    if r["t_support"] > r["t_peel"]:
+                    "device_seconds": t, "launches": launches, "peak_kind": pk,
+                    "definition": "4*sum_e T(e)^2 + 36T + 48Q bytes per full enumeration (zipper bound)"})
+    # the dominant kernel is the one with the larger device time
+    if out[1]["device_seconds"] > out[0]["device_seconds"]:
         out.reverse()
     return out[0], out[1]
 

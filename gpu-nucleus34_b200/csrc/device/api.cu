@@ -227,6 +227,7 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 	bool peeled = false;
 	do
 	{
+		c.peel_debit_sec = 0;
 		N34_CUDA(cudaEventRecord(ev.e[0], c.stream));
 		if ((rc = list_triangles(c)))
 			break;
@@ -317,6 +318,7 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 	r.t_support = ev.sec(2, 3);
 	r.t_cliques = ev.sec(3, 4);
 	r.t_peel = ev.sec(4, 5);
+	r.t_peel_debit = c.peel_debit_sec;
 	r.t_total = r.t_triangles + r.t_incidence + r.t_support + r.t_cliques + r.t_peel;
 	if (peeled)
 	{
@@ -426,7 +428,18 @@ int create_ctx(const nucleus34_opts *opts, nucleus34_ctx *out)
 	}
 	size_t fb = 0, tb = 0;
 	cudaMemGetInfo(&fb, &tb);
-	c.budget = (opts && opts->mem_budget_bytes) ? opts->mem_budget_bytes : uint64_t(double(fb) * 0.9);
+	// memory cached in the pool by earlier calls is available to this one too
+	uint64_t cached = 0;
+	{
+		cudaMemPool_t pool;
+		uint64_t reserved = 0, used = 0;
+		if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+			cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+			cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+			cached = reserved - used;
+		cudaGetLastError();
+	}
+	c.budget = (opts && opts->mem_budget_bytes) ? opts->mem_budget_bytes : uint64_t(double(fb + cached) * 0.9);
 	if (opts && opts->tune_table)
 		c.tune_table = opts->tune_table;
 	if (opts)
@@ -451,12 +464,8 @@ void destroy_ctx(nucleus34_ctx x)
 		cudaStreamSynchronize(c.stream);
 		cudaStreamDestroy(c.stream);
 	}
-	{
-		cudaMemPool_t pool;
-		if (cudaDeviceGetDefaultMemPool(&pool, c.device) == cudaSuccess)
-			cudaMemPoolTrimTo(pool, 0);
-		cudaGetLastError();
-	}
+	// the freed blocks stay cached in the device's pool for the next call;
+	// nucleus34_release_cached_memory returns them to the driver
 	delete x;
 }
 
@@ -604,6 +613,24 @@ int nucleus34_write_kfile(nucleus34_handle h, const char *path)
 	return guarded([&] {
 		std::lock_guard<std::mutex> lk(h->ctx->c.mu);
 		return write_kfile(h->ctx->c, path);
+	});
+}
+
+int nucleus34_release_cached_memory(int device)
+{
+	return guarded([&]() -> int {
+		int ndev = 0;
+		if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+		{
+			cudaGetLastError();
+			return fail(NUCLEUS34_E_NODEVICE, "no CUDA device");
+		}
+		if (device < 0 || device >= ndev)
+			return fail(NUCLEUS34_E_INVALID, "device ordinal out of range");
+		cudaMemPool_t pool;
+		N34_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+		N34_CUDA(cudaMemPoolTrimTo(pool, 0));
+		return NUCLEUS34_OK;
 	});
 }
 

@@ -98,6 +98,7 @@ struct Ctx
 	uint64_t launches = 0;
 	std::string tune_table;
 	uint32_t opt_flags = 0;
+	double peel_debit_sec = 0; // profiling only: debit kernels' device time
 	std::mutex mu;
 
 	// resident graph

@@ -69,33 +69,72 @@ __device__ __forceinline__ bool use_merge(const Lists &L)
 	return (L.b1 - L.b0) <= MERGE_RATIO * (L.a1 - L.a0);
 }
 
-// Warp lower bounds: every lane with want gets the first position in [lo, hi)
-// whose entry is >= its x (hi if none). Called by all lanes. Long ranges are
-// first narrowed to 1/32 by a sample of 32 evenly spaced entries loaded at
-// once, so the per-lane binary searches start five levels down.
-__device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi,
-													 bool want, uint32_t x)
+// L2 prefetch of a list range by the bulk-copy engine (one instruction per
+// 64 KB, issued by one lane): later tile loads of a long list then hit L2
+// instead of DRAM. The range is widened to 16-byte boundaries, which stay
+// inside the array because allocations are 256-byte aligned and padded.
+#ifndef N34_L2_PREFETCH_MIN
+#define N34_L2_PREFETCH_MIN 64u
+#endif
+__device__ __forceinline__ void prefetch_range_l2(const uint32_t *base, uint32_t lo, uint32_t hi)
 {
-	const uint32_t n = hi - lo;
-	uint32_t l = lo, h = hi;
-	if (n >= N34_SAMPLE_MIN) // warp-uniform
+	if (hi - lo < N34_L2_PREFETCH_MIN)
+		return;
+	uintptr_t a = reinterpret_cast<uintptr_t>(base + lo) & ~uintptr_t(15);
+	const uintptr_t e = (reinterpret_cast<uintptr_t>(base + hi) + 15) & ~uintptr_t(15);
+	while (a < e)
 	{
-		const uint32_t lane = lane_id();
+		const uint32_t n = uint32_t((e - a) > 65536 ? 65536 : (e - a));
+		asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(n) : "memory");
+		a += n;
+	}
+}
+
+// Warp lower bounds: every lane with want gets the first position in [lo, hi)
+// whose entry is >= its x (hi if none). Long ranges are first narrowed to
+// 1/32 by a sample of 32 evenly spaced entries loaded at once, so the
+// per-lane binary searches start five levels down. A sample of a list can be
+// taken once and reused while the searched range only moves forward.
+struct WarpSample
+{
+	uint32_t sp; // sample position of this lane (end of slice lane)
+	uint32_t sv; // entry there
+	bool on;     // range long enough to be sampled (warp-uniform)
+};
+
+__device__ __forceinline__ WarpSample warp_sample(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi)
+{
+	WarpSample s{0u, 0u, (hi - lo) >= N34_SAMPLE_MIN};
+	if (s.on)
+	{
+		const uint32_t n = hi - lo;
 		// sample i sits at the end of slice i: lo + ceil(n * (i+1) / 32) - 1
-		const uint32_t sp = lo + uint32_t((uint64_t(n) * (lane + 1) + 31) >> 5) - 1;
-		const uint32_t sv = __ldg(a + sp);
-		// first sample >= x (32 if none)
+		s.sp = lo + uint32_t((uint64_t(n) * (lane_id() + 1) + 31) >> 5) - 1;
+		s.sv = __ldg(a + s.sp);
+	}
+	return s;
+}
+
+// Lower bounds in [lo, hi) using a sample taken over [lo0, hi) with lo0 <= lo
+// (every entry before lo is below every x searched now). Called by all lanes.
+__device__ __forceinline__ uint32_t sampled_lower_bound(const uint32_t *__restrict__ a, const WarpSample &s,
+														uint32_t lo, uint32_t hi, bool want, uint32_t x)
+{
+	uint32_t l = lo, h = hi;
+	if (s.on) // warp-uniform
+	{
+		// first sample >= x (31 if none)
 		uint32_t j = 0;
 #pragma unroll
 		for (uint32_t step = 16; step > 0; step >>= 1)
 		{
-			const uint32_t probe = __shfl_sync(FULL, sv, (j + step - 1) & 31);
+			const uint32_t probe = __shfl_sync(FULL, s.sv, (j + step - 1) & 31);
 			if (probe < x)
 				j += step;
 		}
-		const uint32_t last = __shfl_sync(FULL, sv, 31);
-		const uint32_t sj = __shfl_sync(FULL, sp, j & 31);
-		const uint32_t sprev = __shfl_sync(FULL, sp, (j + 31) & 31);
+		const uint32_t last = __shfl_sync(FULL, s.sv, 31);
+		const uint32_t sj = __shfl_sync(FULL, s.sp, j & 31);
+		const uint32_t sprev = __shfl_sync(FULL, s.sp, (j + 31) & 31);
 		if (last < x)
 		{
 			l = hi;
@@ -103,16 +142,21 @@ __device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t *__restrict_
 		}
 		else
 		{
-			l = j ? sprev + 1 : lo;
-			h = sj; // a[sj] >= x: the bound is at most sj
+			const uint32_t from = j ? sprev + 1 : lo;
+			l = from > lo ? from : lo;
+			h = sj; // a[sj] >= x: the bound is at most sj (and at least lo)
 		}
 	}
 	uint32_t r = hi;
 	if (want)
-	{
 		r = lower_bound32(a, l, h, x);
-	}
 	return r;
+}
+
+__device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi,
+													 bool want, uint32_t x)
+{
+	return sampled_lower_bound(a, warp_sample(a, lo, hi), lo, hi, want, x);
 }
 
 // Warp tile merge of A and B. f(found, x, pa, pb, qa, qb) is called by all

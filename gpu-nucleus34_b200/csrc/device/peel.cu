@@ -25,6 +25,7 @@
 //   advance            swap frontiers, advance the round.
 // The result is independent of thread timing: ownership depends only on the
 // stamps, and crossing detection catches every triangle that reaches the level.
+#include <algorithm>
 #include <cstdio>
 #include <vector>
 
@@ -549,8 +550,11 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 // resolved 32 entries at a time (each lane one lookup on the longest list),
 // so the dependent search chain is paid once per 32 live cliques instead of
 // once per merge step that has any.
+#ifndef N34_L2_PREFETCH
+#define N34_L2_PREFETCH 1
+#endif
 #ifndef N34_DEBIT_MINB
-#define N34_DEBIT_MINB 8
+#define N34_DEBIT_MINB 6
 #endif
 __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
@@ -577,25 +581,37 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 <= THREAD_MODE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
+#if N34_L2_PREFETCH
+		if (lane == 0 && use_merge(L))
+		{
+			prefetch_range_l2(third, L.a0, L.a1);
+			prefetch_range_l2(third, L.b0, L.b1);
+			prefetch_range_l2(itri, L.a0, L.a1);
+			prefetch_range_l2(itri, L.b0, L.b1);
+		}
+#endif
 		uint32_t lo_c = L.c0;
 		uint32_t queued = 0; // warp-uniform
+		// one sample of C serves every resolve of this triangle
+		const WarpSample cs = warp_sample(third, L.c0, L.c1);
 		// resolves the first n (<= 32) queued entries; called by all lanes
 		auto resolve = [&](uint32_t n) {
 			__syncwarp();
 			const bool v = lane < n;
 			const uint32_t x = v ? bx[lane] : 0xffffffffu;
 			const uint32_t q0 = v ? b0[lane] : DEAD, q1 = v ? b1[lane] : DEAD;
-			const uint32_t pc = warp_lower_bound(third, lo_c, L.c1, v, x);
+			const uint32_t pc = sampled_lower_bound(third, cs, lo_c, L.c1, v, x);
 			lo_c = __shfl_sync(FULL, pc, n - 1); // thirds ascend through the queue
 			bool hit[3] = {false, false, false};
-			uint32_t q2 = DEAD;
-			// absent from C: that partner died and was compacted away (clique destroyed)
-			if (v && pc < L.c1 && __ldg(third + pc) == x)
+			uint32_t q2 = DEAD, xc = 0xffffffffu;
+			if (v && pc < L.c1)
 			{
+				xc = __ldg(third + pc);
 				q2 = __ldg(itri + pc);
-				if (!(q2 & DEAD))
-					settle_flags(t, q0, q1, q2, S, level, hit);
 			}
+			// absent from C: that partner died and was compacted away (clique destroyed)
+			if (v && xc == x && !(q2 & DEAD))
+				settle_flags(t, q0, q1, q2, S, level, hit);
 			const uint32_t qs[3] = {q0, q1, q2};
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
@@ -613,7 +629,10 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 		};
 		warp_intersect2<true>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
 												  uint32_t qb) {
-			const bool live = found && !(qa & DEAD) && !(qb & DEAD);
+			// a clique is looked up on C only if its partners on A and B are
+			// alive and neither is a dying triangle of smaller id (its owner)
+			const bool live = found && !(qa & DEAD) && !(qb & DEAD) &&
+							  !((qa & DYING) && (qa & ID_MASK) < t) && !((qb & DYING) && (qb & ID_MASK) < t);
 			const uint32_t fm = __ballot_sync(FULL, live);
 			if (!fm)
 				return;
@@ -650,6 +669,183 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 		if (queued)
 			resolve(queued);
 		__syncwarp();
+	}
+}
+
+// Ordering of large frontiers. Appends leave the next frontier in random
+// order; the debit of a random order reads every dying triangle's lists from
+// DRAM, while in id order (edge-major, as the triangles are numbered)
+// neighbouring warps share lists in L2. A frontier of at least T >> SORT_SHIFT
+// triangles is therefore rewritten in id order through a bitmap: set bits,
+// count per chunk, scan the counts, write the ids back (clearing the bits).
+#ifndef N34_SORT_SHIFT
+#define N34_SORT_SHIFT 12
+#endif
+#ifndef N34_SORT_MIN
+#define N34_SORT_MIN 4096ull
+#endif
+constexpr uint32_t SORT_CHUNK_WORDS = 1024; // bitmap words per chunk (4 per thread)
+constexpr int SORT_THREADS = 256;
+
+__device__ __forceinline__ bool sort_wanted(const CtlX *ctl, uint64_t T)
+{
+	const uint64_t thr = (T >> N34_SORT_SHIFT) > N34_SORT_MIN ? (T >> N34_SORT_SHIFT) : N34_SORT_MIN;
+	return !ctl->c.done && ctl->c.nNext >= thr && ctl->c.nNext <= T;
+}
+
+__global__ void k_fsort_set(const CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
+							uint32_t *__restrict__ bits, uint64_t T)
+{
+	if (!sort_wanted(ctl, T))
+		return;
+	const uint32_t *Fn = ctl->c.cur ? F0 : F1;
+	const uint32_t n = ctl->c.nNext;
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
+	{
+		const uint32_t t = Fn[i];
+		if (t < T)
+			atomicOr(bits + (t >> 5), 1u << (t & 31));
+	}
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_fsort_count(const CtlX *ctl, const uint32_t *__restrict__ bits,
+															   uint64_t W, uint32_t *__restrict__ chunk, uint64_t T)
+{
+	if (!sort_wanted(ctl, T))
+		return;
+	const uint64_t nchunks = (W + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
+	__shared__ uint32_t wsum[SORT_THREADS / 32];
+	for (uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
+	{
+		uint32_t cnt = 0;
+#pragma unroll
+		for (int k = 0; k < 4; ++k)
+		{
+			const uint64_t w = ch * SORT_CHUNK_WORDS + uint64_t(k) * SORT_THREADS + threadIdx.x;
+			if (w < W)
+				cnt += __popc(bits[w]);
+		}
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1)
+			cnt += __shfl_xor_sync(FULL, cnt, o);
+		if (lane_id() == 0)
+			wsum[threadIdx.x >> 5] = cnt;
+		__syncthreads();
+		if (threadIdx.x == 0)
+		{
+			uint32_t tot = 0;
+			for (int i = 0; i < SORT_THREADS / 32; ++i)
+				tot += wsum[i];
+			chunk[ch] = tot;
+		}
+		__syncthreads();
+	}
+}
+
+// exclusive scan of the chunk counts, one block
+__global__ void __launch_bounds__(1024) k_fsort_scan(const CtlX *ctl, uint32_t *__restrict__ chunk, uint64_t nchunks,
+													  uint64_t T)
+{
+	if (!sort_wanted(ctl, T))
+		return;
+	__shared__ uint32_t part[32];
+	__shared__ uint32_t carry;
+	if (threadIdx.x == 0)
+		carry = 0;
+	__syncthreads();
+	for (uint64_t base = 0; base < nchunks; base += 1024)
+	{
+		const uint64_t i = base + threadIdx.x;
+		const uint32_t v = i < nchunks ? chunk[i] : 0u;
+		uint32_t x = v; // inclusive warp scan
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			const uint32_t y = __shfl_up_sync(FULL, x, o);
+			if (lane_id() >= uint32_t(o))
+				x += y;
+		}
+		if (lane_id() == 31)
+			part[threadIdx.x >> 5] = x;
+		__syncthreads();
+		if (threadIdx.x < 32)
+		{
+			uint32_t p = part[threadIdx.x];
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1)
+			{
+				const uint32_t y = __shfl_up_sync(FULL, p, o);
+				if (lane_id() >= uint32_t(o))
+					p += y;
+			}
+			part[threadIdx.x] = p; // inclusive over warps
+		}
+		__syncthreads();
+		const uint32_t wbase = (threadIdx.x >> 5) ? part[(threadIdx.x >> 5) - 1] : 0u;
+		if (i < nchunks)
+			chunk[i] = carry + wbase + x - v;
+		__syncthreads();
+		if (threadIdx.x == 0)
+			carry += part[31];
+		__syncthreads();
+	}
+}
+
+__global__ void __launch_bounds__(SORT_THREADS) k_fsort_write(const CtlX *ctl, uint32_t *__restrict__ bits,
+															   uint64_t W, const uint32_t *__restrict__ chunk,
+															   uint32_t *__restrict__ F0, uint32_t *__restrict__ F1,
+															   uint64_t T)
+{
+	if (!sort_wanted(ctl, T))
+		return;
+	uint32_t *Fn = ctl->c.cur ? F0 : F1;
+	const uint32_t n = ctl->c.nNext;
+	const uint64_t nchunks = (W + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
+	__shared__ uint32_t wsum[SORT_THREADS / 32];
+	for (uint64_t ch = blockIdx.x; ch < nchunks; ch += gridDim.x)
+	{
+		// each thread owns 4 consecutive words so that its ids come out in order
+		const uint64_t w0 = ch * SORT_CHUNK_WORDS + 4 * uint64_t(threadIdx.x);
+		uint32_t wv[4];
+		uint32_t cnt = 0;
+#pragma unroll
+		for (int k = 0; k < 4; ++k)
+		{
+			wv[k] = (w0 + k < W) ? bits[w0 + k] : 0u;
+			cnt += __popc(wv[k]);
+		}
+		uint32_t x = cnt; // inclusive block scan of the thread counts
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1)
+		{
+			const uint32_t y = __shfl_up_sync(FULL, x, o);
+			if (lane_id() >= uint32_t(o))
+				x += y;
+		}
+		if (lane_id() == 31)
+			wsum[threadIdx.x >> 5] = x;
+		__syncthreads();
+		uint32_t wb = 0;
+		for (uint32_t i = 0; i < (threadIdx.x >> 5); ++i)
+			wb += wsum[i];
+		uint32_t pos = chunk[ch] + wb + x - cnt;
+#pragma unroll
+		for (int k = 0; k < 4; ++k)
+		{
+			uint32_t m = wv[k];
+			while (m)
+			{
+				const uint32_t b = __ffs(m) - 1;
+				m &= m - 1;
+				if (pos < n)
+					Fn[pos] = uint32_t((w0 + k) * 32 + b);
+				++pos;
+			}
+			if (wv[k])
+				bits[w0 + k] = 0u;
+		}
+		__syncthreads();
 	}
 }
 
@@ -778,7 +974,7 @@ __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_t *S, int32_t *K, PeelCtl *hctl)
 {
 	const uint64_t T = c.T;
-	uint32_t *R = nullptr, *F0 = nullptr, *F1 = nullptr;
+	uint32_t *R = nullptr, *F0 = nullptr, *F1 = nullptr, *fbits = nullptr, *fchunk = nullptr;
 	uint8_t *destroyed = nullptr;
 	CtlX *ctl = nullptr;
 	int rc = NUCLEUS34_OK;
@@ -786,6 +982,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		c.release(R);
 		c.release(F0);
 		c.release(F1);
+		c.release(fbits);
+		c.release(fchunk);
 		c.release(ctl);
 		c.release(destroyed);
 	};
@@ -799,6 +997,23 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			break;
 		if ((rc = dalloc(c, &ctl, 1, "peel control")))
 			break;
+		// frontier ordering bitmap (optional: skipped without room for it)
+		const uint64_t fwords = (T + 31) / 32;
+		const uint64_t fchunks = (fwords + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
+		if (dalloc(c, &fbits, fwords, "frontier order bitmap") || dalloc(c, &fchunk, fchunks, "frontier order chunks"))
+		{
+			c.release(fbits);
+			c.release(fchunk);
+			fbits = nullptr;
+			fchunk = nullptr;
+			clear_error();
+		}
+		else if (cudaMemsetAsync(fbits, 0, fwords * 4, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "memset");
+			break;
+		}
+		const uint32_t gsort = uint32_t(std::min<uint64_t>(fchunks, uint64_t(c.sm_count) * 8));
 		if (variant == NUCLEUS34_DIRECT)
 		{
 			if ((rc = dalloc(c, &destroyed, c.Q ? c.Q : 1, "clique destroyed flags")))
@@ -822,7 +1037,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		const bool profile = (c.opt_flags & NUCLEUS34_OPT_PROFILE_PEEL) != 0;
 		constexpr int PROF_STEPS = 8;
 		static const char *const prof_names[PROF_STEPS] = {"gather_next", "scan_min", "gather",	   "mark",
-														   "debit_thread", "debit_warp", "finalize", "advance"};
+														   "debit_thread", "debit_warp", "finalize", "order+advance"};
 		// One round = a fixed kernel sequence that reads its sizes from ctl.
 		auto launch_round = [&](cudaEvent_t *ev, uint32_t *trace) {
 			auto tick = [&](int j) {
@@ -868,11 +1083,18 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				tick(6);
 				tick(7);
 			}
+			if (fbits)
+			{
+				k_fsort_set<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, fbits, T);
+				k_fsort_count<<<gsort, SORT_THREADS, 0, c.stream>>>(ctl, fbits, fwords, fchunk, T);
+				k_fsort_scan<<<1, 1024, 0, c.stream>>>(ctl, fchunk, fchunks, T);
+				k_fsort_write<<<gsort, SORT_THREADS, 0, c.stream>>>(ctl, fbits, fwords, fchunk, F0, F1, T);
+			}
 			k_advance<<<1, 1, 0, c.stream>>>(ctl);
 			if (ev)
 				cudaEventRecord(ev[PROF_STEPS], c.stream);
 		};
-		const uint32_t per_round = flags ? 8u : 6u;
+		const uint32_t per_round = (flags ? 8u : 6u) + (fbits ? 4u : 0u);
 		// Rounds are replayed from a CUDA graph of ROUNDS_PER_GRAPH rounds; the
 		// host reads the control block once per replay. Rounds after the last
 		// one are no-ops.
@@ -1021,6 +1243,9 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			for (int j = 0; j < PROF_STEPS; ++j)
 				std::fprintf(stderr, " %s=%.1fms", prof_names[j], prof_ms[j]);
 			std::fprintf(stderr, "\n");
+			// steps 4 and 5: the debit kernels (thread + warp, or the single
+			// stamp/direct debit in slot 4)
+			c.peel_debit_sec = (prof_ms[4] + prof_ms[5]) * 1e-3;
 		}
 		if (exec)
 			cudaGraphExecDestroy(exec);

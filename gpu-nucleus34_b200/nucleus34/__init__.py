@@ -44,7 +44,7 @@ _VARIANTS = {"direct": DIRECT, "ondemand": ONDEMAND, DIRECT: DIRECT, ONDEMAND: O
 # Every symbol include/nucleus34.h declares (checked by the CPU test suite).
 EXPORTED = (
     "nucleus34_decompose", "nucleus34_decompose_ondemand", "nucleus34_copy_k",
-    "nucleus34_copy_quds", "nucleus34_write_kfile", "nucleus34_free",
+    "nucleus34_copy_quds", "nucleus34_write_kfile", "nucleus34_free", "nucleus34_release_cached_memory",
     "nucleus34_strerror", "nucleus34_last_error",
     "nucleus34_ctx_create", "nucleus34_ctx_upload", "nucleus34_ctx_run",
     "nucleus34_ctx_copy_k", "nucleus34_ctx_destroy",
@@ -83,7 +83,7 @@ class Result(C.Structure):
                 ("t_peel", C.c_double), ("t_total", C.c_double),
                 ("incidence_entries", C.c_uint64), ("gpu_launches", C.c_uint64),
                 ("peak_device_bytes", C.c_uint64), ("variant", C.c_int),
-                ("sum_te_sq", C.c_uint64)]
+                ("sum_te_sq", C.c_uint64), ("t_peel_debit", C.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -128,6 +128,8 @@ def lib() -> C.CDLL:
     L.nucleus34_write_kfile.restype = C.c_int
     L.nucleus34_free.argtypes = [C.c_void_p]
     L.nucleus34_free.restype = None
+    L.nucleus34_release_cached_memory.argtypes = [C.c_int]
+    L.nucleus34_release_cached_memory.restype = C.c_int
     L.nucleus34_ctx_create.argtypes = [C.POINTER(Opts), C.POINTER(C.c_void_p)]
     L.nucleus34_ctx_create.restype = C.c_int
     L.nucleus34_ctx_upload.argtypes = [C.c_void_p, C.POINTER(Csr)]

@@ -103,6 +103,9 @@ typedef struct
 	int variant;                  /* NUCLEUS34_DIRECT or NUCLEUS34_ONDEMAND */
 	uint64_t sum_te_sq;           /* sum over edges of T(e)^2, T(e) = triangles on edge e
 	                                 (work measure of the 3-way intersections) */
+	/* with NUCLEUS34_OPT_PROFILE_PEEL only (0 otherwise): device time of the
+	 * peel's re-enumeration kernels summed over all rounds, seconds */
+	double t_peel_debit;
 } nucleus34_result;
 
 typedef struct nucleus34_state *nucleus34_handle;
@@ -134,7 +137,14 @@ int nucleus34_copy_quds(nucleus34_handle h, uint64_t first, uint64_t count, uint
  * canonical order (layout of cuNucleus34_ondemand.cu:724-733). */
 int nucleus34_write_kfile(nucleus34_handle h, const char *path);
 
+/* Releases the handle's device memory into the device's stream-ordered pool,
+ * where it stays cached for later calls (re-mapping tens of GB would cost more
+ * than the decomposition); nucleus34_release_cached_memory hands it back. */
 void nucleus34_free(nucleus34_handle h);
+
+/* Returns the device memory cached by earlier calls (the default memory pool
+ * of `device`, trimmed to zero) to the driver. */
+int nucleus34_release_cached_memory(int device);
 
 const char *nucleus34_strerror(int code);
 /* Detail of the calling thread's last failure ("" if none). */
