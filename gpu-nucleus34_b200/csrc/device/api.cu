@@ -19,11 +19,6 @@
 
 #include <omp.h>
 
-struct nucleus34_ctx_s
-{
-	n34::Ctx c;
-};
-
 struct nucleus34_state
 {
 	nucleus34_ctx ctx = nullptr;
@@ -134,6 +129,14 @@ void Ctx::release(void *p)
 
 void Ctx::release_results()
 {
+	release(dseg);
+	dseg = nullptr;
+	seg_toff.clear();
+	seg_q.clear();
+	seg_ksum.clear();
+	seg_kmax.clear();
+	release(dR);
+	dR = nullptr;
 	release(dtris);
 	release(dK);
 	release(dquds);
@@ -162,6 +165,7 @@ int upload(Ctx &c, const nucleus34_csr *csr)
 	N34_TRY(set_device(c));
 	c.release_results();
 	c.release_graph();
+	c.seg_eoff.clear();
 	const uint64_t n = csr->n, m = csr->m;
 	std::vector<uint32_t> O(n + 1);
 	uint64_t s = 0;
@@ -231,6 +235,8 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 		N34_CUDA(cudaEventRecord(ev.e[0], c.stream));
 		if ((rc = list_triangles(c)))
 			break;
+		if ((rc = segments_after_listing(c)))
+			break;
 		N34_CUDA(cudaEventRecord(ev.e[1], c.stream));
 		r.triangle_count = c.T;
 		r.incidence_entries = 3 * c.T;
@@ -247,7 +253,8 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 			// the on-demand peel with death flags (T < 2^30) keeps each
 			// triangle's entry positions
 			const bool want_tpos =
-				variant == NUCLEUS34_ONDEMAND && c.T <= 0x3fffffffull && !(c.opt_flags & NUCLEUS34_OPT_STAMP_PEEL);
+				variant == NUCLEUS34_ONDEMAND && c.T <= 0x3fffffffull &&
+				!(c.opt_flags & (NUCLEUS34_OPT_STAMP_PEEL | NUCLEUS34_OPT_LEAN_MEMORY));
 			if ((rc = build_incidence(c, inc, want_tpos)))
 				break;
 			r.sum_te_sq = inc.sum_te_sq;
@@ -268,6 +275,8 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 				break;
 			}
 		}
+		if ((rc = segments_after_support(c, S)))
+			break;
 		r.four_clique_count = total / 4;
 		N34_CUDA(cudaEventRecord(ev.e[3], c.stream));
 		if (variant == NUCLEUS34_DIRECT && total)
@@ -301,6 +310,8 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 			}
 		}
 		N34_CUDA(cudaEventRecord(ev.e[5], c.stream));
+		if ((rc = segments_after_peel(c)))
+			break;
 		N34_CUDA(cudaStreamSynchronize(c.stream));
 	} while (false);
 	free_incidence(c, inc);
@@ -566,6 +577,16 @@ int nucleus34_ctx_copy_k(nucleus34_ctx ctx, int32_t *k_out, uint32_t *tris_out)
 }
 
 void nucleus34_ctx_destroy(nucleus34_ctx ctx) { destroy_ctx(ctx); }
+
+int nucleus34_ctx_verify(nucleus34_ctx ctx, uint64_t *violations, uint64_t *checked)
+{
+	if (!ctx || !violations || !checked)
+		return fail(NUCLEUS34_E_INVALID, "null argument");
+	return guarded([&] {
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		return verify(ctx->c, violations, checked);
+	});
+}
 
 int nucleus34_decompose(const nucleus34_csr *csr, const nucleus34_opts *opts, nucleus34_result *res,
 						nucleus34_handle *out)

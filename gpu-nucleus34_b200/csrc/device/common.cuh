@@ -114,7 +114,17 @@ struct Ctx
 	uint32_t *dtris = nullptr; // 3T
 	int32_t *dK = nullptr;     // T
 	uint32_t *dquds = nullptr; // 4Q (direct)
+	uint32_t *dR = nullptr;    // T death rounds (kept with NUCLEUS34_OPT_VERIFIABLE)
 	nucleus34_result res{};
+
+	// Segments (batched graphs decomposed as one disjoint union): seg_eoff
+	// holds count+1 edge offsets of the member graphs; empty for a single
+	// graph. After a run the per-segment triangle offsets, clique counts and
+	// k statistics are in the host vectors.
+	std::vector<uint64_t> seg_eoff;
+	std::vector<uint64_t> seg_toff, seg_q, seg_ksum;
+	std::vector<uint32_t> seg_kmax;
+	uint64_t *dseg = nullptr; // device: eoff (count+1), toff (count+1), q, ksum (count), kmax (count, u32 words)
 
 	std::unordered_map<void *, uint64_t> sizes; // live allocations
 

@@ -418,19 +418,23 @@ __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const u
 							 int32_t *__restrict__ K, int32_t *__restrict__ S, const uint32_t *__restrict__ tris,
 							 const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
 							 const uint2 *__restrict__ span, const uint32_t *__restrict__ third,
-							 const uint32_t *__restrict__ tpos, uint32_t *__restrict__ itri, uint64_t n3)
+							 const uint32_t *__restrict__ tpos, uint32_t *__restrict__ itri, uint64_t n3,
+							 uint32_t *__restrict__ R)
 {
 	if (ctl->c.done)
 		return;
 	const uint32_t nF = ctl->c.nF;
 	const uint32_t *F = ctl->c.cur ? F1 : F0;
 	const int32_t level = int32_t(ctl->c.level);
+	const uint32_t round = ctl->c.round;
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nF; i += stride)
 	{
 		const uint32_t t = F[i];
 		K[t] = level;
 		S[t] = INT32_MAX;
+		if (R)
+			R[t] = round;
 		uint64_t pos[3];
 		entry_positions(t, tris, src, E, span, third, tpos, pos);
 #pragma unroll
@@ -987,9 +991,15 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		c.release(ctl);
 		c.release(destroyed);
 	};
+	// death flags live in the incidence entries when triangle ids leave the
+	// top two bits free (the incidence is discarded after the peel)
+	const bool flags = variant == NUCLEUS34_ONDEMAND && T <= ID_MASK && !(c.opt_flags & NUCLEUS34_OPT_STAMP_PEEL);
+	// death rounds: the round-stamp owner test needs them; the death-flag
+	// path records them only to keep them for nucleus34_ctx_verify
+	const bool keep_rounds = (c.opt_flags & NUCLEUS34_OPT_VERIFIABLE) != 0;
 	do
 	{
-		if ((rc = dalloc(c, &R, T, "peel round stamps")))
+		if ((!flags || keep_rounds) && (rc = dalloc(c, &R, T, "peel round stamps")))
 			break;
 		if ((rc = dalloc(c, &F0, T, "frontier 0")))
 			break;
@@ -1000,7 +1010,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		// frontier ordering bitmap (optional: skipped without room for it)
 		const uint64_t fwords = (T + 31) / 32;
 		const uint64_t fchunks = (fwords + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
-		if (dalloc(c, &fbits, fwords, "frontier order bitmap") || dalloc(c, &fchunk, fchunks, "frontier order chunks"))
+		if ((c.opt_flags & NUCLEUS34_OPT_LEAN_MEMORY) || dalloc(c, &fbits, fwords, "frontier order bitmap") ||
+			dalloc(c, &fchunk, fchunks, "frontier order chunks"))
 		{
 			c.release(fbits);
 			c.release(fchunk);
@@ -1024,10 +1035,6 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				break;
 			}
 		}
-		// death flags live in the incidence entries when triangle ids leave the
-		// top two bits free (the incidence is discarded after the peel)
-		const bool flags =
-			variant == NUCLEUS34_ONDEMAND && T <= ID_MASK && !(c.opt_flags & NUCLEUS34_OPT_STAMP_PEEL);
 		const uint32_t gscan = grid_for(c, T, PEEL_THREADS, 8);
 		const uint32_t gwarp = grid_for(c, T, PEEL_THREADS / 32, 16);
 		k_peel_init<<<gscan, PEEL_THREADS, 0, c.stream>>>(K, T, ctl);
@@ -1056,7 +1063,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			if (flags)
 			{
 				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.span,
-																   inc.third, inc.tpos, inc.tri, 3 * T);
+																   inc.third, inc.tpos, inc.tri, 3 * T, R);
 				tick(4);
 				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.span,
 																		   inc.third, inc.tri, S, T);
@@ -1266,6 +1273,11 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			rc = fail(NUCLEUS34_E_CUDA, "internal: peel check failed (" +
 									   std::string(hctl->error & 2u ? "compaction bound" : "frontier overflow") + ")");
 			break;
+		}
+		if (keep_rounds)
+		{
+			c.dR = R; // kept for nucleus34_ctx_verify
+			R = nullptr;
 		}
 	} while (false);
 	cleanup();

@@ -46,8 +46,27 @@ int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *tota
 // Direct variant: canonical clique list (c.dquds, c.Q) and triangle->clique CSR.
 int list_cliques(Ctx &c, const Incidence &inc, const int32_t *support, const uint32_t *own, CliqueCsr &csr);
 void free_clique_csr(Ctx &c, CliqueCsr &csr);
+// Per-segment statistics of a batched (disjoint union) run; no-ops when the
+// context holds a single graph. After listing: triangle offsets per member
+// graph; after the support count: clique counts; after the peel: k max/sum.
+int segments_after_listing(Ctx &c);
+int segments_after_support(Ctx &c, const int32_t *support);
+int segments_after_peel(Ctx &c);
 // Device-resident peel; K receives the final k of every triangle.
 int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_t *support, int32_t *K,
 		 PeelCtl *hctl);
 
+// Certificate check of the last run (verify.cu); needs the kept death rounds.
+int verify(Ctx &c, uint64_t *violations, uint64_t *checked);
+// Context entry points shared by the C-ABI front ends (api.cu, batch.cu).
+int upload(Ctx &c, const nucleus34_csr *csr);
+int run(Ctx &c, int variant, nucleus34_result *out);
+int create_ctx(const nucleus34_opts *opts, nucleus34_ctx *out);
+void destroy_ctx(nucleus34_ctx x);
+
 } // namespace n34
+
+struct nucleus34_ctx_s
+{
+	n34::Ctx c;
+};

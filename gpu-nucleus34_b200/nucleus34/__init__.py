@@ -45,9 +45,10 @@ _VARIANTS = {"direct": DIRECT, "ondemand": ONDEMAND, DIRECT: DIRECT, ONDEMAND: O
 EXPORTED = (
     "nucleus34_decompose", "nucleus34_decompose_ondemand", "nucleus34_copy_k",
     "nucleus34_copy_quds", "nucleus34_write_kfile", "nucleus34_free", "nucleus34_release_cached_memory",
+    "nucleus34_batch_decompose", "nucleus34_batch_summary", "nucleus34_batch_copy_k", "nucleus34_batch_free",
     "nucleus34_strerror", "nucleus34_last_error",
     "nucleus34_ctx_create", "nucleus34_ctx_upload", "nucleus34_ctx_run",
-    "nucleus34_ctx_copy_k", "nucleus34_ctx_destroy",
+    "nucleus34_ctx_copy_k", "nucleus34_ctx_destroy", "nucleus34_ctx_verify",
     "nucleus34_graph_load", "nucleus34_graph_from_edges", "nucleus34_graph_save_grh",
     "nucleus34_graph_release", "nucleus34_graph_csr",
     "nucleus34_gen_rmat", "nucleus34_gen_rgg", "nucleus34_gen_ws",
@@ -87,6 +88,24 @@ class Result(C.Structure):
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class BatchResult(C.Structure):
+    _fields_ = [("graphs", C.c_uint64), ("triangle_count", C.c_uint64), ("four_clique_count", C.c_uint64),
+                ("peeling_iterations", C.c_uint64), ("t_upload", C.c_double), ("t_triangles", C.c_double),
+                ("t_incidence", C.c_double), ("t_support", C.c_double), ("t_peel", C.c_double),
+                ("t_total", C.c_double), ("gpu_launches", C.c_uint64), ("peak_device_bytes", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class GraphSummary(C.Structure):
+    _fields_ = [("triangle_count", C.c_uint64), ("four_clique_count", C.c_uint64), ("k_max", C.c_uint32),
+                ("k_avg", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class Graph(C.Structure):
@@ -130,6 +149,15 @@ def lib() -> C.CDLL:
     L.nucleus34_free.restype = None
     L.nucleus34_release_cached_memory.argtypes = [C.c_int]
     L.nucleus34_release_cached_memory.restype = C.c_int
+    L.nucleus34_batch_decompose.argtypes = [C.POINTER(Csr), C.c_uint64, C.POINTER(Opts), C.POINTER(BatchResult),
+                                            C.POINTER(C.c_void_p)]
+    L.nucleus34_batch_decompose.restype = C.c_int
+    L.nucleus34_batch_summary.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(GraphSummary)]
+    L.nucleus34_batch_summary.restype = C.c_int
+    L.nucleus34_batch_copy_k.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_int32), u32p]
+    L.nucleus34_batch_copy_k.restype = C.c_int
+    L.nucleus34_batch_free.argtypes = [C.c_void_p]
+    L.nucleus34_batch_free.restype = None
     L.nucleus34_ctx_create.argtypes = [C.POINTER(Opts), C.POINTER(C.c_void_p)]
     L.nucleus34_ctx_create.restype = C.c_int
     L.nucleus34_ctx_upload.argtypes = [C.c_void_p, C.POINTER(Csr)]
@@ -138,6 +166,8 @@ def lib() -> C.CDLL:
     L.nucleus34_ctx_run.restype = C.c_int
     L.nucleus34_ctx_copy_k.argtypes = [C.c_void_p, C.POINTER(C.c_int32), u32p]
     L.nucleus34_ctx_copy_k.restype = C.c_int
+    L.nucleus34_ctx_verify.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.nucleus34_ctx_verify.restype = C.c_int
     L.nucleus34_ctx_destroy.argtypes = [C.c_void_p]
     L.nucleus34_ctx_destroy.restype = None
     L.nucleus34_graph_load.argtypes = [C.c_char_p, C.POINTER(Graph)]
@@ -278,6 +308,8 @@ class Decomposition:
 
 OPT_STAMP_PEEL = 0x1
 OPT_PROFILE_PEEL = 0x2
+OPT_LEAN_MEMORY = 0x4
+OPT_VERIFIABLE = 0x8
 
 
 def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1, flags: int = 0) -> Opts:
@@ -314,6 +346,57 @@ def decompose(g: HostGraph, variant="direct", device: int = 0, mem_budget_bytes:
         L.nucleus34_free(h)
 
 
+class Batch:
+    """Results of nucleus34_batch_decompose: one shared device pass over many graphs."""
+
+    def __init__(self, handle: C.c_void_p, result: dict, count: int):
+        self._L = lib()
+        self._h = handle
+        self.result = result
+        self.count = count
+
+    def summary(self, i: int) -> dict:
+        s = GraphSummary()
+        _check(self._L.nucleus34_batch_summary(self._h, i, C.byref(s)), "batch_summary")
+        return s.as_dict()
+
+    def copy_k(self, i: int, with_tris: bool = False):
+        T = self.summary(i)["triangle_count"]
+        k = np.zeros(T, np.int32)
+        tris = np.zeros(3 * T, np.uint32) if with_tris else None
+        _check(self._L.nucleus34_batch_copy_k(self._h, i, k.ctypes.data_as(C.POINTER(C.c_int32)),
+                                              _u32p(tris) if tris is not None else None), "batch_copy_k")
+        return (k, tris.reshape(-1, 3)) if with_tris else k
+
+    def close(self) -> None:
+        if self._h:
+            self._L.nucleus34_batch_free(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_decompose(graphs, device: int = 0, mem_budget_bytes: int = 0, flags: int = 0) -> Batch:
+    """Decomposes a list of HostGraph in one device pass (nucleus34_batch_decompose)."""
+    L = lib()
+    arr = (Csr * len(graphs))(*[g.csr() for g in graphs])
+    opts = make_opts(device, mem_budget_bytes, flags=flags)
+    res = BatchResult()
+    h = C.c_void_p()
+    _check(L.nucleus34_batch_decompose(arr, len(graphs), C.byref(opts), C.byref(res), C.byref(h)), "batch_decompose")
+    return Batch(h, res.as_dict(), len(graphs))
+
+
 class Context:
     """Device-resident context: upload once, run many times."""
 
@@ -340,6 +423,12 @@ class Context:
             self._h, k.ctypes.data_as(C.POINTER(C.c_int32)),
             _u32p(tris) if tris is not None else None), "ctx_copy_k")
         return (k, tris.reshape(-1, 3)) if with_tris else k
+
+    def verify(self) -> tuple:
+        """(violations, checked) of nucleus34_ctx_verify for the last run."""
+        v, n = C.c_uint64(), C.c_uint64()
+        _check(self._L.nucleus34_ctx_verify(self._h, C.byref(v), C.byref(n)), "ctx_verify")
+        return int(v.value), int(n.value)
 
     def close(self) -> None:
         if self._h:

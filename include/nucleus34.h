@@ -81,6 +81,14 @@ typedef struct
  * every step and print per-step device times to stderr (diagnostics only;
  * slower than the default graph replay). */
 #define NUCLEUS34_OPT_PROFILE_PEEL 0x2u
+/* opts.flags: allocate none of the optional speed-up arrays (per-triangle
+ * entry positions, frontier-order bitmap); the peel then searches for a
+ * triangle's entries and keeps frontiers in append order. The same arrays
+ * are skipped automatically when the memory budget has no room for them. */
+#define NUCLEUS34_OPT_LEAN_MEMORY 0x4u
+/* opts.flags: keep each triangle's death round after the peel, so that
+ * nucleus34_ctx_verify can certify the result (costs 4 bytes per triangle). */
+#define NUCLEUS34_OPT_VERIFIABLE 0x8u
 
 typedef struct
 {
@@ -162,6 +170,52 @@ int nucleus34_ctx_upload(nucleus34_ctx ctx, const nucleus34_csr *csr);
 int nucleus34_ctx_run(nucleus34_ctx ctx, int variant, nucleus34_result *res);
 int nucleus34_ctx_copy_k(nucleus34_ctx ctx, int32_t *k_out, uint32_t *tris_out);
 void nucleus34_ctx_destroy(nucleus34_ctx ctx);
+/* Certifies the last run's k (needs NUCLEUS34_OPT_VERIFIABLE): every
+ * triangle t must lie in at least k(t) cliques whose triangles all have
+ * k >= k(t), must have had at most k(t) cliques with all partners alive when
+ * its round began, and the level must never decrease from round to round.
+ * Together these hold exactly for the (3,4)-nucleus numbers. *violations
+ * receives the number of triangles (and rounds) that fail; *checked the
+ * number of triangles examined. Rebuilds the edge->triangle incidence. */
+int nucleus34_ctx_verify(nucleus34_ctx ctx, uint64_t *violations, uint64_t *checked);
+
+/* ---- batched decomposition ------------------------------------------------ */
+
+/* Many independent graphs decomposed in one device pass (their disjoint
+ * union: one listing, incidence, support count and peel for the whole
+ * batch). Every graph's triangle list, counts and k equal those of
+ * nucleus34_decompose_ondemand on that graph alone. No reference
+ * counterpart: the reference decomposes one graph per process. */
+typedef struct nucleus34_batch_s *nucleus34_batch;
+
+typedef struct
+{
+	uint64_t graphs;
+	uint64_t triangle_count;      /* over all graphs */
+	uint64_t four_clique_count;   /* over all graphs */
+	uint64_t peeling_iterations;  /* rounds of the shared peel */
+	double t_upload;              /* host union build + upload, seconds (wall) */
+	double t_triangles, t_incidence, t_support, t_peel;
+	double t_total;               /* device time of the shared pass */
+	uint64_t gpu_launches;
+	uint64_t peak_device_bytes;
+} nucleus34_batch_result;
+
+typedef struct
+{
+	uint64_t triangle_count;
+	uint64_t four_clique_count;
+	uint32_t k_max;
+	double k_avg;                 /* sum(k) / T in 64-bit integers, as for one graph */
+} nucleus34_graph_summary;
+
+int nucleus34_batch_decompose(const nucleus34_csr *graphs, uint64_t count, const nucleus34_opts *opts,
+							  nucleus34_batch_result *res, nucleus34_batch *out);
+int nucleus34_batch_summary(nucleus34_batch b, uint64_t index, nucleus34_graph_summary *out);
+/* Graph `index`'s k in its canonical order and, if tris_out is not NULL, its
+ * triangles as (a,b,c) edge ids of that graph alone. */
+int nucleus34_batch_copy_k(nucleus34_batch b, uint64_t index, int32_t *k_out, uint32_t *tris_out);
+void nucleus34_batch_free(nucleus34_batch b);
 
 /* ---- triangle listing without allocation --------------------------------- */
 

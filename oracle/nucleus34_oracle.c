@@ -454,6 +454,71 @@ uint64_t oracle_count_triangles(const oracle_graph *g)
 	return T;
 }
 
+/* Four-clique count by oriented neighbourhoods, independent of the
+ * edge->triangle incidence and of any peel: with the degree orientation every
+ * four-clique has exactly one vertex u that points to the other three, and
+ * among those one v that points to the other two, and so on; so it is counted
+ * once as u -> v -> w (a triangle of u's out-lists) plus an x in
+ * N+(u) & N+(v) & N+(w). Used as an independent check of the clique totals on
+ * graphs too large for the full oracle (no counterpart in the reference). */
+static uint64_t count3(const uint32_t *a, uint32_t na, const uint32_t *b, uint32_t nb, const uint32_t *c,
+					   uint32_t nc)
+{
+	uint64_t cnt = 0;
+	uint32_t i = 0, j = 0, k = 0;
+	while (i < na && j < nb && k < nc)
+	{
+		const uint32_t x = a[i], y = b[j], z = c[k];
+		if (x == y && y == z)
+		{
+			++cnt;
+			++i, ++j, ++k;
+			continue;
+		}
+		const uint32_t mx = x > y ? (x > z ? x : z) : (y > z ? y : z);
+		if (x < mx)
+			++i;
+		if (y < mx)
+			++j;
+		if (z < mx)
+			++k;
+	}
+	return cnt;
+}
+
+uint64_t oracle_count_k4(const oracle_graph *g)
+{
+	uint64_t Q = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : Q)
+	for (uint64_t u = 0; u < g->n; ++u)
+	{
+		const uint32_t *nu = g->E + g->O[u];
+		const uint32_t du = g->O[u + 1] - g->O[u];
+		for (uint32_t i = 0; i < du; ++i)
+		{
+			const uint32_t v = nu[i];
+			const uint32_t *nv = g->E + g->O[v];
+			const uint32_t dv = g->O[v + 1] - g->O[v];
+			/* w in N+(u) & N+(v) */
+			uint32_t p = 0, q = 0;
+			while (p < du && q < dv)
+			{
+				if (nu[p] < nv[q])
+					++p;
+				else if (nu[p] > nv[q])
+					++q;
+				else
+				{
+					const uint32_t w = nu[p];
+					Q += count3(nu, du, nv, dv, g->E + g->O[w], g->O[w + 1] - g->O[w]);
+					++p, ++q;
+				}
+			}
+		}
+	}
+	return Q;
+}
+
 /* canonical order: tuple sort on (a,b) (graph.hpp:108, helpers.hpp:305-317;
  * tri_t::operator< utils.cuh:98-101). Since a and b are both out-edges of the
  * same vertex u, the order is u-major; sort within each vertex's block. */

@@ -61,6 +61,8 @@ void oracle_result_free(oracle_result *r);
 
 /* Triangle count only (listing without storage). */
 uint64_t oracle_count_triangles(const oracle_graph *g);
+/* four-cliques counted by oriented neighbourhoods (independent of the incidence) */
+uint64_t oracle_count_k4(const oracle_graph *g);
 
 #ifdef __cplusplus
 }

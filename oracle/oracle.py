@@ -59,6 +59,8 @@ def lib():
         L.oracle_result_free.restype = None
         L.oracle_count_triangles.argtypes = [C.POINTER(OGraph)]
         L.oracle_count_triangles.restype = C.c_uint64
+        L.oracle_count_k4.argtypes = [C.POINTER(OGraph)]
+        L.oracle_count_k4.restype = C.c_uint64
         _LIB = L
     return _LIB
 
@@ -143,3 +145,20 @@ def kfile_bytes(tris: np.ndarray, k: np.ndarray) -> bytes:
     """Rows "(a,b,c)\\t<k>\\n" as the programs write them."""
     lines = [f"({a},{b},{c})\t{kk}\n" for (a, b, c), kk in zip(tris.tolist(), k.tolist())]
     return "".join(lines).encode()
+
+
+def count_k4(g) -> int:
+    """Four-cliques of the oriented CSR g, counted by oriented neighbourhoods
+    (independent of the incidence-based support count)."""
+    D = np.ascontiguousarray(g.D, np.uint32)
+    E = np.ascontiguousarray(g.E if g.m else np.zeros(1, np.uint32), np.uint32)
+    og = OGraph()
+    L = lib()
+    rc = L.oracle_graph_from_oriented(int(g.n), int(g.m), D.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                      E.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(og))
+    if rc:
+        raise RuntimeError(f"oracle_graph_from_oriented = {rc}")
+    try:
+        return int(L.oracle_count_k4(C.byref(og)))
+    finally:
+        L.oracle_graph_free(C.byref(og))

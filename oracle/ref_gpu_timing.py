@@ -13,6 +13,10 @@ free, and the reference takes its segmented path by its own rule.
 
     python oracle/ref_gpu_timing.py --scale 18 --program ondemand
     python oracle/ref_gpu_timing.py --scale 20 --program ondemand --free-gb 80
+    python oracle/ref_gpu_timing.py --graph rgg --n 4000000 --degree 48 --seed 3
+
+With --compare the same graph also goes through libnucleus34's one-shot call
+and the record's counts, K_max, K_avg and first k values are compared.
 """
 import argparse
 import json
@@ -39,7 +43,11 @@ time.sleep(3600)
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--scale", type=int, required=True)
+    ap.add_argument("--graph", choices=["rmat", "rgg"], default="rmat")
+    ap.add_argument("--scale", type=int, default=12)
+    ap.add_argument("--n", type=int, default=4000000)
+    ap.add_argument("--degree", type=float, default=48.0)
+    ap.add_argument("--compare", action="store_true")
     ap.add_argument("--edge-factor", type=int, default=16)
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--program", choices=["ondemand", "direct"], default="ondemand")
@@ -50,10 +58,17 @@ def main():
     exe = os.path.join(HERE, "_ref", "cuNucleus34_ondemand" if a.program == "ondemand" else "cuNucleus34")
     if not os.path.exists(exe):
         sys.exit(f"{exe} missing (make -C oracle ref)")
-    out = {"scale": a.scale, "edge_factor": a.edge_factor, "seed": a.seed, "program": os.path.basename(exe)}
+    if a.graph == "rmat":
+        out = {"graph": "rmat", "scale": a.scale, "edge_factor": a.edge_factor, "seed": a.seed}
+    else:
+        out = {"graph": "rgg", "n": a.n, "degree": a.degree, "seed": a.seed}
+    out["program"] = os.path.basename(exe)
     with tempfile.TemporaryDirectory() as td:
-        path = os.path.join(td, f"rmat{a.scale}.edges")
-        s, d = n34.gen_rmat(a.scale, a.edge_factor, a.seed)
+        path = os.path.join(td, "graph.edges")
+        if a.graph == "rmat":
+            s, d = n34.gen_rmat(a.scale, a.edge_factor, a.seed)
+        else:
+            s, d = n34.gen_rgg(a.n, a.degree, a.seed)
         n34.write_edges(s, d, path)
         side = None
         try:
@@ -77,6 +92,23 @@ def main():
             if side is not None:
                 side.terminate()
                 side.wait(timeout=30)
+        if a.compare and "record" in out:
+            g = n34.load_graph(path)
+            dec = n34.decompose(g, variant=a.program, n_quds=0)
+            rec, res = out["record"], dec.result
+            kref = [int(x) for x in rec.get("K", [])]
+            ours = {"triangle_count": int(res["triangle_count"]), "four_clique_count": int(res["four_clique_count"]),
+                    "K_max": int(res["k_max"]), "K_avg": float(res["k_avg"]), "t_total": float(res["t_total"]),
+                    "K": [int(x) for x in dec.k[:len(kref)]]}
+            out["ours"] = ours
+            out["equal"] = {
+                "triangle_count": int(rec.get("triangle_count", -1)) == ours["triangle_count"],
+                "four_clique_count": int(rec.get("four_clique_count", -1)) == ours["four_clique_count"],
+                "K_max": int(rec.get("K_max", -1)) == ours["K_max"],
+                # the record prints K_avg with 6 significant digits
+                "K_avg": float(f"{ours['K_avg']:.6g}") == float(rec.get("K_avg", -1)),
+                "K_first": kref == ours["K"],
+            }
     print(json.dumps(out), flush=True)
 
 

@@ -1,0 +1,64 @@
+"""Batched decomposition (nucleus34_batch_decompose): many graphs in one
+device pass as their disjoint union. Every graph's triangles, counts, K_max,
+K_avg and k must equal its own one-graph decomposition and the oracle, bit
+for bit (integer results; K_avg uses the same 64-bit sum / T)."""
+import numpy as np
+import pytest
+
+
+def _mixed_graphs(n34, count, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        kind = i % 4
+        s = n34.splitmix64(seed * 1000 + i) & 0xffffffff
+        if kind == 0:
+            a, b = n34.gen_rmat(int(rng.integers(6, 11)), int(rng.integers(8, 20)), s)
+        elif kind == 1:
+            a, b = n34.gen_ws(int(rng.integers(200, 3000)), 10, 0.1, s)
+        elif kind == 2:
+            a, b = n34.gen_rgg(int(rng.integers(500, 4000)), float(rng.integers(16, 40)), s)
+        else:
+            a, b = n34.gen_rmat(int(rng.integers(4, 9)), int(rng.integers(4, 12)), s)
+        out.append(n34.graph_from_edges(a, b))
+    return out
+
+
+def test_batch_rejects_bad_members_before_any_device_work(n34):
+    a, b = n34.gen_rmat(6, 8, 1)
+    g = n34.graph_from_edges(a, b)
+    bad = n34.HostGraph(g.n, g.m, g.O.copy(), g.D.copy(), g.E.copy())
+    bad.E[0] = g.n + 5
+    with pytest.raises(n34.Nucleus34Error) as ei:
+        n34.batch_decompose([g, bad])
+    assert ei.value.code == n34.E_INVALID
+    assert "batch graph 1" in n34.last_error()
+    with pytest.raises(n34.Nucleus34Error):
+        n34.batch_decompose([])
+
+
+@pytest.mark.gpu
+def test_batch_equals_single_graph_runs_and_oracle(n34, oracle):
+    graphs = _mixed_graphs(n34, 24, 4)
+    # edge cases inside a batch: an empty graph and a triangle-free path
+    graphs.insert(5, n34.graph_from_edges(np.zeros(0, np.uint32), np.zeros(0, np.uint32)))
+    graphs.insert(9, n34.graph_from_edges(np.arange(0, 50, dtype=np.uint32), np.arange(1, 51, dtype=np.uint32)))
+    with n34.batch_decompose(graphs) as b:
+        assert b.result["graphs"] == len(graphs)
+        tot_t = tot_q = 0
+        for i, g in enumerate(graphs):
+            one = n34.decompose(g, variant="ondemand", n_quds=0)
+            summ = b.summary(i)
+            k, tris = b.copy_k(i, with_tris=True)
+            assert summ["triangle_count"] == one.result["triangle_count"]
+            assert summ["four_clique_count"] == one.result["four_clique_count"]
+            assert summ["k_max"] == one.result["k_max"]
+            assert summ["k_avg"] == one.result["k_avg"]
+            assert np.array_equal(k, one.k)
+            assert np.array_equal(tris, one.tris)
+            o = oracle.decompose(g, quds_cap=0)
+            assert np.array_equal(k, o.k) and summ["four_clique_count"] == o.Q
+            tot_t += summ["triangle_count"]
+            tot_q += summ["four_clique_count"]
+        assert tot_t == b.result["triangle_count"]
+        assert tot_q == b.result["four_clique_count"]

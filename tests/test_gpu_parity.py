@@ -112,3 +112,20 @@ def test_stamp_peel_path_matches(n34, oracle, case):
     o = oracle.decompose(g)
     assert np.array_equal(d.k, o.k)
     assert d.result["four_clique_count"] == o.Q
+
+
+@pytest.mark.parametrize("case", [("rmat", 13, 16, 3), ("rgg", 30000, 40, 9)])
+def test_lean_and_profiled_peels_match(n34, oracle, case):
+    """Without the optional arrays (entries searched, frontiers unordered) and
+    with the per-step profiling launches, k is the same."""
+    if case[0] == "rmat":
+        s, t = n34.gen_rmat(case[1], case[2], case[3])
+    else:
+        s, t = n34.gen_rgg(case[1], case[2], case[3])
+    g = n34.graph_from_edges(s, t)
+    o = oracle.decompose(g)
+    lean = n34.decompose(g, variant="ondemand", flags=n34.OPT_LEAN_MEMORY)
+    assert np.array_equal(lean.k, o.k)
+    prof = n34.decompose(g, variant="ondemand", flags=n34.OPT_PROFILE_PEEL)
+    assert np.array_equal(prof.k, o.k)
+    assert prof.result["t_peel_debit"] > 0
