@@ -24,11 +24,20 @@
 #include <string>
 #include <vector>
 
-struct nucleus34_batch_s
+// A batch is split into chunks whose unions stay within the 32-bit entry
+// positions of the incidence (3T < 2^32); each chunk is one device pass in
+// its own context, and its results stay resident until nucleus34_batch_free.
+struct BatchChunk
 {
 	nucleus34_ctx ctx = nullptr;
+	uint64_t first = 0, count = 0; // member graphs [first, first + count)
+};
+
+struct nucleus34_batch_s
+{
+	std::vector<BatchChunk> chunks;
+	std::vector<uint32_t> chunk_of; // graph -> chunk
 	uint64_t count = 0;
-	std::vector<uint64_t> voff; // vertex offsets (count+1)
 };
 
 namespace n34 {
@@ -101,6 +110,25 @@ __global__ void k_seg_kstats(const int32_t *__restrict__ K, const uint64_t *__re
 			ksum[g] = acc;
 			kmax[g] = mx;
 		}
+	}
+}
+
+// triangles per member graph from per-vertex counts (warp per graph)
+__global__ void k_seg_vertex_sums(const uint32_t *__restrict__ cnt, const uint64_t *__restrict__ voff, uint64_t count,
+								  unsigned long long *__restrict__ out)
+{
+	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+	for (uint64_t g = warp; g < count; g += nwarps)
+	{
+		unsigned long long acc = 0;
+		for (uint64_t u = voff[g] + lane_id(); u < voff[g + 1]; u += 32)
+			acc += cnt[u];
+#pragma unroll
+		for (int o = 16; o > 0; o >>= 1)
+			acc += __shfl_xor_sync(FULL, acc, o);
+		if (lane_id() == 0)
+			out[g] = acc;
 	}
 }
 
@@ -227,6 +255,57 @@ int build_union(const nucleus34_csr *graphs, uint64_t count, std::vector<uint32_
 	return NUCLEUS34_OK;
 }
 
+// Triangles of every member graph: the listing's count pass over the union
+// already uploaded to c, summed per graph.
+int triangles_per_graph(Ctx &c, const std::vector<uint64_t> &voff, std::vector<uint64_t> &tcount)
+{
+	const uint64_t count = voff.size() - 1;
+	tcount.assign(count, 0);
+	if (!c.m)
+		return NUCLEUS34_OK;
+	uint32_t *cnt = nullptr;
+	uint64_t *dv = nullptr;
+	unsigned long long *dout = nullptr;
+	int rc = NUCLEUS34_OK;
+	do
+	{
+		if ((rc = dalloc(c, &cnt, c.n, "batch triangle counts")) || (rc = dalloc(c, &dv, count + 1, "batch offsets")) ||
+			(rc = dalloc(c, &dout, count, "batch sums")))
+			break;
+		if (launch_tri_count(c.dO, c.dE, c.n, cnt, c.sm_count, c.stream) != cudaSuccess ||
+			cudaMemcpyAsync(dv, voff.data(), (count + 1) * 8, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "batch triangle count");
+			break;
+		}
+		k_seg_vertex_sums<<<grid_for(c, count, 8), 256, 0, c.stream>>>(cnt, dv, count, dout);
+		c.launches += 2;
+		if (cudaMemcpyAsync(tcount.data(), dout, count * 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+			rc = fail(NUCLEUS34_E_CUDA, "batch triangle count");
+	} while (false);
+	c.release(cnt);
+	c.release(dv);
+	c.release(dout);
+	return rc;
+}
+
+// Union of the member graphs [first, last) of the full union (O, D, E),
+// re-based to start at vertex 0 and edge 0.
+void slice_union(const std::vector<uint32_t> &O, const std::vector<uint32_t> &D, const std::vector<uint32_t> &E,
+				 const std::vector<uint64_t> &voff, const std::vector<uint64_t> &eoff, uint64_t first, uint64_t last,
+				 std::vector<uint32_t> &So, std::vector<uint32_t> &Sd, std::vector<uint32_t> &Se)
+{
+	const uint64_t v0 = voff[first], v1 = voff[last], e0 = eoff[first], e1 = eoff[last];
+	So.resize(v1 - v0 + 1);
+	Sd.assign(D.begin() + v0, D.begin() + v1);
+	Se.resize(e1 - e0);
+	for (uint64_t u = v0; u <= v1; ++u)
+		So[u - v0] = uint32_t(O[u] - e0);
+	for (uint64_t j = e0; j < e1; ++j)
+		Se[j - e0] = uint32_t(E[j] - v0);
+}
+
 } // namespace n34
 
 using namespace n34;
@@ -262,82 +341,166 @@ int nucleus34_batch_decompose(const nucleus34_csr *graphs, uint64_t count, const
 		std::vector<uint32_t> O, D, E;
 		std::vector<uint64_t> voff, eoff;
 		N34_TRY(build_union(graphs, count, O, D, E, voff, eoff));
-		nucleus34_ctx ctx = nullptr;
-		N34_TRY(create_ctx(opts, &ctx));
 		auto *b = new (std::nothrow) nucleus34_batch_s();
 		if (!b)
-		{
-			destroy_ctx(ctx);
 			return fail(NUCLEUS34_E_OOM_BUDGET, "host allocation failed");
-		}
-		b->ctx = ctx;
 		b->count = count;
-		b->voff = voff;
-		Ctx &c = ctx->c;
-		const nucleus34_csr u{voff[count], eoff[count], O.data(), D.data(), E.empty() ? nullptr : E.data()};
-		int rc = upload(c, &u);
-		const double t_upload =
-			std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
-		nucleus34_result r{};
-		if (!rc)
+		b->chunk_of.assign(count, 0);
+		nucleus34_batch_result br{};
+		br.graphs = count;
+		double t_upload = 0;
+		auto finish = [&](int rc) {
+			if (rc)
+				nucleus34_batch_free(b);
+			return rc;
+		};
+		// pass 0: the whole union, counted per graph
+		nucleus34_ctx ctx0 = nullptr;
+		int rc = create_ctx(opts, &ctx0);
+		if (rc)
+			return finish(rc);
 		{
-			c.seg_eoff = eoff;
-			rc = run(c, NUCLEUS34_ONDEMAND, &r);
+			const nucleus34_csr u{voff[count], eoff[count], O.data(), D.data(), E.empty() ? nullptr : E.data()};
+			rc = upload(ctx0->c, &u);
 		}
+		std::vector<uint64_t> tcount;
+		if (!rc)
+			rc = triangles_per_graph(ctx0->c, voff, tcount);
 		if (rc)
 		{
-			nucleus34_batch_free(b);
-			return rc;
+			destroy_ctx(ctx0);
+			return finish(rc);
 		}
-		if (res)
+		// chunks: greedy in graph order, 3T < 2^32 entry positions each, and
+		// about PASS_BYTES_PER_TRIANGLE bytes of a pass's peak per triangle
+		// within the memory budget (a single graph over that still runs alone)
+		constexpr uint64_t PASS_BYTES_PER_TRIANGLE = 80;
+		const uint64_t range_limit = 0xffffffffull / 3;
+		const uint64_t csr_bytes = 4 * (voff[count] + 1) + 8 * eoff[count];
+		const uint64_t budget = ctx0->c.budget;
+		const uint64_t mem_limit = budget > csr_bytes ? (budget - csr_bytes) / PASS_BYTES_PER_TRIANGLE : 0;
+		const uint64_t limit = std::max<uint64_t>(1, std::min(range_limit, mem_limit));
+		std::vector<uint64_t> cut{0};
+		uint64_t acc = 0;
+		for (uint64_t g = 0; g < count; ++g)
 		{
-			nucleus34_batch_result br{};
-			br.graphs = count;
-			br.triangle_count = r.triangle_count;
-			br.four_clique_count = r.four_clique_count;
-			br.peeling_iterations = r.peeling_iterations;
-			br.t_upload = t_upload;
-			br.t_triangles = r.t_triangles;
-			br.t_incidence = r.t_incidence;
-			br.t_support = r.t_support;
-			br.t_peel = r.t_peel;
-			br.t_total = r.t_total;
-			br.gpu_launches = r.gpu_launches;
-			br.peak_device_bytes = r.peak_device_bytes;
-			*res = br;
+			if (tcount[g] > range_limit)
+			{
+				destroy_ctx(ctx0);
+				return finish(fail(NUCLEUS34_E_RANGE32, "batch graph " + std::to_string(g) + " alone has " +
+															 std::to_string(tcount[g]) + " triangles (incidence "
+															 "exceeds the 32-bit position range)"));
+			}
+			if (acc && acc + tcount[g] > limit)
+			{
+				cut.push_back(g);
+				acc = 0;
+			}
+			acc += tcount[g];
 		}
+		cut.push_back(count);
+		const uint64_t nchunks = cut.size() - 1;
+		t_upload += std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
+		for (uint64_t ci = 0; ci < nchunks; ++ci)
+		{
+			const uint64_t f = cut[ci], l = cut[ci + 1];
+			const auto c0 = std::chrono::steady_clock::now();
+			nucleus34_ctx ctx = nullptr;
+			if (nchunks == 1)
+			{
+				ctx = ctx0; // the union is already resident
+				ctx0 = nullptr;
+			}
+			else
+			{
+				if (ctx0)
+				{
+					destroy_ctx(ctx0);
+					ctx0 = nullptr;
+				}
+				if ((rc = create_ctx(opts, &ctx)))
+					return finish(rc);
+				std::vector<uint32_t> So, Sd, Se;
+				slice_union(O, D, E, voff, eoff, f, l, So, Sd, Se);
+				const nucleus34_csr u{voff[l] - voff[f], eoff[l] - eoff[f], So.data(), Sd.data(),
+									  Se.empty() ? nullptr : Se.data()};
+				if ((rc = upload(ctx->c, &u)))
+				{
+					destroy_ctx(ctx);
+					return finish(rc);
+				}
+			}
+			b->chunks.push_back(BatchChunk{ctx, f, l - f});
+			for (uint64_t g = f; g < l; ++g)
+				b->chunk_of[g] = uint32_t(ci);
+			Ctx &c = ctx->c;
+			c.seg_eoff.resize(l - f + 1);
+			for (uint64_t g = f; g <= l; ++g)
+				c.seg_eoff[g - f] = eoff[g] - eoff[f];
+			t_upload += std::chrono::duration<double>(std::chrono::steady_clock::now() - c0).count();
+			nucleus34_result r{};
+			if ((rc = run(c, NUCLEUS34_ONDEMAND, &r)))
+				return finish(rc);
+			br.triangle_count += r.triangle_count;
+			br.four_clique_count += r.four_clique_count;
+			br.peeling_iterations += r.peeling_iterations;
+			br.t_triangles += r.t_triangles;
+			br.t_incidence += r.t_incidence;
+			br.t_support += r.t_support;
+			br.t_peel += r.t_peel;
+			br.t_total += r.t_total;
+			br.gpu_launches += r.gpu_launches;
+			br.peak_device_bytes = std::max<uint64_t>(br.peak_device_bytes, r.peak_device_bytes);
+		}
+		br.t_upload = t_upload;
+		br.chunks = nchunks;
+		if (res)
+			*res = br;
 		*out = b;
 		return int(NUCLEUS34_OK);
 	});
 }
 
+static const BatchChunk *chunk_for(nucleus34_batch b, uint64_t index, uint64_t *local)
+{
+	if (!b || index >= b->count)
+		return nullptr;
+	const BatchChunk &ch = b->chunks[b->chunk_of[index]];
+	*local = index - ch.first;
+	return &ch;
+}
+
 int nucleus34_batch_summary(nucleus34_batch b, uint64_t index, nucleus34_graph_summary *out)
 {
-	if (!b || !b->ctx || !out)
-		return fail(NUCLEUS34_E_INVALID, "null argument");
-	const Ctx &c = b->ctx->c;
-	if (index >= b->count || c.seg_toff.size() != b->count + 1)
-		return fail(NUCLEUS34_E_INVALID, "graph index out of range");
+	uint64_t i = 0;
+	const BatchChunk *ch = chunk_for(b, index, &i);
+	if (!ch || !out)
+		return fail(NUCLEUS34_E_INVALID, "null argument or graph index out of range");
+	const Ctx &c = ch->ctx->c;
+	if (c.seg_toff.size() != ch->count + 1)
+		return fail(NUCLEUS34_E_STATE, "batch has no result");
 	nucleus34_graph_summary s{};
-	s.triangle_count = c.seg_toff[index + 1] - c.seg_toff[index];
-	s.four_clique_count = c.seg_q[index];
-	s.k_max = c.seg_kmax[index];
+	s.triangle_count = c.seg_toff[i + 1] - c.seg_toff[i];
+	s.four_clique_count = c.seg_q[i];
+	s.k_max = c.seg_kmax[i];
 	// same arithmetic as a single decomposition: 64-bit integer sum / T
-	s.k_avg = s.triangle_count ? double(c.seg_ksum[index]) / double(s.triangle_count) : 0.0;
+	s.k_avg = s.triangle_count ? double(c.seg_ksum[i]) / double(s.triangle_count) : 0.0;
 	*out = s;
 	return NUCLEUS34_OK;
 }
 
 int nucleus34_batch_copy_k(nucleus34_batch b, uint64_t index, int32_t *k_out, uint32_t *tris_out)
 {
-	if (!b || !b->ctx)
-		return fail(NUCLEUS34_E_INVALID, "null argument");
+	uint64_t i = 0;
+	const BatchChunk *ch = chunk_for(b, index, &i);
+	if (!ch)
+		return fail(NUCLEUS34_E_INVALID, "null argument or graph index out of range");
 	return batch_guarded([&]() -> int {
-		Ctx &c = b->ctx->c;
+		Ctx &c = ch->ctx->c;
 		std::lock_guard<std::mutex> lk(c.mu);
-		if (index >= b->count || c.seg_toff.size() != b->count + 1)
-			return fail(NUCLEUS34_E_INVALID, "graph index out of range");
-		const uint64_t t0 = c.seg_toff[index], T = c.seg_toff[index + 1] - t0;
+		if (c.seg_toff.size() != ch->count + 1)
+			return fail(NUCLEUS34_E_STATE, "batch has no result");
+		const uint64_t t0 = c.seg_toff[i], T = c.seg_toff[i + 1] - t0;
 		if (!T)
 			return int(NUCLEUS34_OK);
 		N34_CUDA(cudaSetDevice(c.device));
@@ -349,9 +512,9 @@ int nucleus34_batch_copy_k(nucleus34_batch b, uint64_t index, int32_t *k_out, ui
 		if (tris_out)
 		{
 			// edge ids of the graph alone
-			const uint32_t eo = uint32_t(c.seg_eoff[index]);
-			for (uint64_t i = 0; i < 3 * T; ++i)
-				tris_out[i] -= eo;
+			const uint32_t eo = uint32_t(c.seg_eoff[i]);
+			for (uint64_t j = 0; j < 3 * T; ++j)
+				tris_out[j] -= eo;
 		}
 		return int(NUCLEUS34_OK);
 	});
@@ -361,7 +524,8 @@ void nucleus34_batch_free(nucleus34_batch b)
 {
 	if (!b)
 		return;
-	destroy_ctx(b->ctx);
+	for (auto &ch : b->chunks)
+		destroy_ctx(ch.ctx);
 	delete b;
 }
 

@@ -94,7 +94,8 @@ class BatchResult(C.Structure):
     _fields_ = [("graphs", C.c_uint64), ("triangle_count", C.c_uint64), ("four_clique_count", C.c_uint64),
                 ("peeling_iterations", C.c_uint64), ("t_upload", C.c_double), ("t_triangles", C.c_double),
                 ("t_incidence", C.c_double), ("t_support", C.c_double), ("t_peel", C.c_double),
-                ("t_total", C.c_double), ("gpu_launches", C.c_uint64), ("peak_device_bytes", C.c_uint64)]
+                ("t_total", C.c_double), ("gpu_launches", C.c_uint64), ("peak_device_bytes", C.c_uint64),
+                ("chunks", C.c_uint64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -183,7 +183,8 @@ int nucleus34_ctx_verify(nucleus34_ctx ctx, uint64_t *violations, uint64_t *chec
 
 /* Many independent graphs decomposed in one device pass (their disjoint
  * union: one listing, incidence, support count and peel for the whole
- * batch). Every graph's triangle list, counts and k equal those of
+ * batch; a batch beyond 2^32/3 triangles is cut into several such passes,
+ * after one counting pass over the whole union). Every graph's triangle list, counts and k equal those of
  * nucleus34_decompose_ondemand on that graph alone. No reference
  * counterpart: the reference decomposes one graph per process. */
 typedef struct nucleus34_batch_s *nucleus34_batch;
@@ -198,7 +199,8 @@ typedef struct
 	double t_triangles, t_incidence, t_support, t_peel;
 	double t_total;               /* device time of the shared pass */
 	uint64_t gpu_launches;
-	uint64_t peak_device_bytes;
+	uint64_t peak_device_bytes;   /* largest pass */
+	uint64_t chunks;              /* device passes: unions are cut so that 3T < 2^32 each */
 } nucleus34_batch_result;
 
 typedef struct

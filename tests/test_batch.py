@@ -62,3 +62,29 @@ def test_batch_equals_single_graph_runs_and_oracle(n34, oracle):
             tot_q += summ["four_clique_count"]
         assert tot_t == b.result["triangle_count"]
         assert tot_q == b.result["four_clique_count"]
+
+
+@pytest.mark.gpu
+def test_batch_cut_into_passes_by_memory_budget(n34):
+    """A budget too small for one union cuts the batch into several passes;
+    results are unchanged."""
+    graphs = _mixed_graphs(n34, 16, 7)
+    single = [n34.decompose(g, variant="ondemand", n_quds=0) for g in graphs]
+    T = sum(int(d.result["triangle_count"]) for d in single)
+    csr = sum(4 * (g.n + 1) + 8 * g.m for g in graphs)
+    done = False
+    for parts in (4, 3, 2):
+        budget = csr + 80 * T // parts + (24 << 20)
+        try:
+            b = n34.batch_decompose(graphs, mem_budget_bytes=budget)
+        except n34.Nucleus34Error as e:
+            assert e.code == n34.E_OOM_BUDGET
+            continue
+        with b:
+            assert b.result["chunks"] >= 2
+            for i, d in enumerate(single):
+                assert np.array_equal(b.copy_k(i), d.k)
+                assert b.summary(i)["four_clique_count"] == d.result["four_clique_count"]
+        done = True
+        break
+    assert done
