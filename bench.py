@@ -61,10 +61,15 @@ def parse():
     p.add_argument("--cpu-sample-scale", type=int, default=14)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="decompose", choices=["decompose", "batch"],
+    p.add_argument("--workload", default="decompose", choices=["decompose", "batch", "serve"],
                    help="decompose: the headline single-graph metric; batch: the batched form "
                         "(graphs/s of nucleus34_batch_decompose vs one decomposition per graph)")
     p.add_argument("--batch-graphs", type=int, default=4096)
+    p.add_argument("--serve-requests", type=int, default=400)
+    p.add_argument("--serve-max-edges", type=float, default=1e6)
+    p.add_argument("--serve-master-seed", type=int, default=5)
+    p.add_argument("--serve-load", default="0.5,1,2,4",
+                   help="arrival rates as multiples of the serial plain capacity")
     p.add_argument("--batch-master-seed", type=int, default=4)
     return p.parse_args()
 
@@ -253,10 +258,120 @@ def run_batch(a):
     return 0 if mism == 0 else 1
 
 
+def serve_specs(count, master, max_edges):
+    """Serving workload: half R-MAT (a/b/c/d .57/.19/.19/.05), half 2D random
+    geometric graphs with expected degree U[16, 64]; undirected edge counts
+    log-uniform over [1e3, max_edges]; request i's parameters and seed come
+    from splitmix64 of (master, i)."""
+    import math
+    import numpy as np
+    import nucleus34 as n34
+    out = []
+    for i in range(count):
+        s = n34.splitmix64((master << 32) ^ (i + 0x9e3779b9))
+        r = np.random.default_rng(s)
+        m = math.exp(r.uniform(math.log(1e3), math.log(max_edges)))
+        if i % 2 == 0:
+            scale = max(4, int(math.ceil(math.log2(m / 16.0))))
+            ef = max(1, int(round(m / (1 << scale))))
+            out.append(("rmat", scale, ef, s & 0xffffffff))
+        else:
+            deg = float(r.uniform(16, 64))
+            n = max(64, int(round(2 * m / deg)))
+            out.append(("rgg", n, deg, s & 0xffffffff))
+    return out
+
+
+def run_serve(a):
+    """Serving: Poisson arrivals into nucleus34_server (continuous batching,
+    two workers) against serial plain execution (one decomposition per request,
+    FIFO, same arrival times: latencies from the measured service times)."""
+    import numpy as np
+    import torch
+    import nucleus34 as n34
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    graphs = []
+    for kind, x, y, seed in serve_specs(a.serve_requests, a.serve_master_seed, a.serve_max_edges):
+        src, dst = n34.gen_rmat(x, y, seed) if kind == "rmat" else n34.gen_rgg(x, y, seed)
+        graphs.append(n34.graph_from_edges(src, dst))
+    n = len(graphs)
+    log(f"[bench] generated {n} requests in {time.perf_counter() - t0:.1f} s, "
+        f"{sum(g.m for g in graphs)} oriented edges")
+    # serial plain service times (and the reference results)
+    service, alone_k = [], []
+    with n34.Context() as ctx:
+        ctx.upload(graphs[0])
+        ctx.run("ondemand")
+        for g in graphs:
+            w = time.perf_counter()
+            ctx.upload(g)
+            r = ctx.run("ondemand")
+            k = ctx.copy_k(int(r["triangle_count"]))
+            service.append(time.perf_counter() - w)
+            alone_k.append(k)
+    cap = n / sum(service)  # serial plain capacity, requests/s
+    rng = np.random.default_rng(a.serve_master_seed)
+    gaps = rng.exponential(1.0, n)
+    sweeps = []
+    mism = 0
+    for load in [float(x) for x in a.serve_load.split(",")]:
+        rate = load * cap
+        arr = np.cumsum(gaps / rate)
+        # serial plain: FIFO single server
+        done, lat = 0.0, []
+        for i in range(n):
+            start = max(arr[i], done)
+            done = start + service[i]
+            lat.append(done - arr[i])
+        plain = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                 "graphs_per_s": n / (done - arr[0])}
+        # the server, fed in real time
+        with n34.Server(workers=2) as srv:
+            ids = [0] * n
+            w0 = time.perf_counter()
+            for i in range(n):
+                wait = arr[i] - arr[0] - (time.perf_counter() - w0)
+                if wait > 0:
+                    time.sleep(wait)
+                ids[i] = srv.submit(graphs[i])
+            infos = [srv.wait(rid) for rid in ids]
+            end = time.perf_counter() - w0
+            for i, (rid, info) in enumerate(zip(ids, infos)):
+                if not np.array_equal(srv.copy_k(rid, info["triangle_count"]), alone_k[i]):
+                    mism += 1
+            st = srv.stats()
+        slat = [x["latency_seconds"] for x in infos]
+        worst = sorted(range(n), key=lambda i: -slat[i])[:8]
+        log(f"[bench] load {load}: slowest requests (latency, queue, triangles, pass, arrival): " +
+            "; ".join(f"{slat[i]:.3f} {infos[i]['queue_seconds']:.3f} {infos[i]['triangle_count']} "
+                      f"{infos[i]['pass']} {arr[i] - arr[0]:.2f}" for i in worst))
+        served = {"p50_s": float(np.percentile(slat, 50)), "p99_s": float(np.percentile(slat, 99)),
+                  "graphs_per_s": n / end, "passes": int(st["passes"])}
+        sweeps.append({"load": load, "rate_per_s": rate, "server": served, "serial_plain": plain})
+        log(f"[bench] load {load}: server p50 {served['p50_s']:.3f} p99 {served['p99_s']:.3f} "
+            f"{served['graphs_per_s']:.1f}/s ({served['passes']} passes); plain p50 {plain['p50_s']:.3f} "
+            f"p99 {plain['p99_s']:.3f} {plain['graphs_per_s']:.1f}/s")
+    top = sweeps[-1]
+    line = {
+        "metric": "graphs/s and p50/p99 latency (serving)", "value": top["server"]["graphs_per_s"],
+        "unit": "graphs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "int32",
+        "data": "synthetic (seeded R-MAT + 2D random geometric graphs)",
+        "config": {"workload": f"{n} requests, Poisson arrivals, half R-MAT half RGG (degree 16..64), undirected "
+                               f"edges log-uniform 1e3..{a.serve_max_edges:.0e}, master seed {a.serve_master_seed}",
+                   "serial_plain_capacity_per_s": cap},
+        "sweep": sweeps, "k_mismatched_requests": mism,
+    }
+    print(json.dumps(line), flush=True)
+    return 0 if mism == 0 else 1
+
+
 def main():
     a = parse()
     if a.workload == "batch":
         return run_batch(a)
+    if a.workload == "serve":
+        return run_serve(a)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
     local = int(os.environ.get("LOCAL_RANK", "0"))

@@ -46,6 +46,7 @@ struct CtlX
 {
 	PeelCtl c;
 	uint32_t scan;        // 1 while the next frontier must come from a scan
+	uint32_t next_found;  // k_scan_min's snapshot: k_gather_next found a frontier
 	uint32_t compact_now; // set by k_compact_gate for the replay's compaction
 	unsigned long long peeled_at_compact;
 	unsigned long long live_at_compact;
@@ -64,6 +65,7 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
 		z.level = 0xffffffffu; // "-1": the first level change tries level 0
 		ctl->c = z;
 		ctl->scan = 1;
+		ctl->next_found = 0;
 		ctl->compact_now = 0;
 		ctl->peeled_at_compact = 0;
 		ctl->live_at_compact = T;
@@ -99,7 +101,14 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather_next(CtlX *ctl, const i
 
 __global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T)
 {
-	if (ctl->c.done || !ctl->scan || ctl->c.nF)
+	if (ctl->c.done || !ctl->scan)
+		return;
+	// nF is final here (k_gather_next has finished); k_gather, which appends
+	// to nF itself, decides from this snapshot instead of reading nF
+	const uint32_t nf = ctl->c.nF;
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		ctl->next_found = nf != 0;
+	if (nf)
 		return;
 	uint32_t mn = INF;
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
@@ -122,7 +131,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_
 {
 	if (ctl->c.done || !ctl->scan)
 		return;
-	if (ctl->c.nF)
+	if (ctl->next_found)
 	{ // k_gather_next found the frontier at level+1
 		if (blockIdx.x == 0 && threadIdx.x == 0)
 			ctl->c.level = ctl->c.level + 1;

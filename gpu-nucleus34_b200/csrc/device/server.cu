@@ -1,0 +1,469 @@
+// Serving: a request loop that keeps graph state on the device and batches
+// requests continuously (nucleus34_server_*).
+//
+// Each worker owns a context (device, stream, pooled memory). A worker takes
+// the pending requests in arrival order that fit the memory still free in the
+// budget (estimated per request from its CSR) and within the 32-bit entry
+// range, decomposes them in one pass as a disjoint union (the batched form),
+// copies every request's results to the host and signals it. Requests that
+// arrive while passes run are admitted by the next free worker, so with two
+// or more workers their passes overlap on the device. A request that asks
+// for its four-clique list is routed to the direct variant and runs alone.
+// Results do not depend on the mix: a graph's triangles and k in a union
+// equal those of the graph alone (the batched form's argument).
+//
+// The reference has no serving loop; it runs one graph per process.
+#include "pipeline.cuh"
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace n34 {
+int build_union(const nucleus34_csr *graphs, uint64_t count, std::vector<uint32_t> &O, std::vector<uint32_t> &D,
+				std::vector<uint32_t> &E, std::vector<uint64_t> &voff, std::vector<uint64_t> &eoff);
+}
+
+using namespace n34;
+
+namespace {
+
+using clk = std::chrono::steady_clock;
+
+struct Request
+{
+	uint64_t id = 0;
+	uint32_t flags = 0;
+	// owned copy of the CSR
+	uint64_t n = 0, m = 0;
+	std::vector<uint32_t> O, D, E;
+	uint64_t est_bytes = 0;     // admission estimate of the pass memory it needs
+	uint64_t est_triangles = 0; // upper bound (wedges)
+	// result
+	bool done = false;
+	int status = NUCLEUS34_OK;
+	std::string error;
+	nucleus34_graph_summary summary{};
+	std::vector<int32_t> k;
+	std::vector<uint32_t> tris;
+	std::vector<uint32_t> quds;
+	clk::time_point t_submit, t_start, t_done;
+	uint64_t pass = 0; // pass that served it
+};
+
+// Bytes of one pass per triangle (peak: listing, incidence build, support,
+// peel arrays) and per oriented edge (CSR, sources, spans, counts).
+constexpr uint64_t PASS_BYTES_PER_TRIANGLE = 80;
+constexpr uint64_t PASS_BYTES_PER_EDGE = 40;
+constexpr uint64_t DIRECT_BYTES_PER_WEDGE = 96; // clique list + incidence, per wedge bound
+
+} // namespace
+
+struct nucleus34_server_s
+{
+	nucleus34_opts opts{};
+	uint64_t budget = 0;          // bytes shared by all passes in flight
+	uint64_t max_batch = 256;     // graphs per pass
+	std::mutex mu;
+	std::condition_variable cv_work, cv_done;
+	std::deque<std::shared_ptr<Request>> pending;
+	std::map<uint64_t, std::shared_ptr<Request>> all;
+	uint64_t next_id = 1, in_flight_bytes = 0, passes = 0, served = 0, busy_workers = 0;
+	bool stop = false;
+	std::vector<std::thread> workers;
+	std::vector<nucleus34_ctx> ctxs;
+};
+
+namespace {
+
+uint64_t wedge_bound(const uint32_t *D, uint64_t n)
+{
+	uint64_t w = 0;
+	for (uint64_t u = 0; u < n; ++u)
+		w += uint64_t(D[u]) * (D[u] ? D[u] - 1 : 0) / 2;
+	return w;
+}
+
+// one pass over a set of on-demand requests (their union) on context c
+void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch)
+{
+	std::vector<nucleus34_csr> csrs(batch.size());
+	for (size_t i = 0; i < batch.size(); ++i)
+		csrs[i] = nucleus34_csr{batch[i]->n, batch[i]->m, batch[i]->O.data(), batch[i]->D.data(),
+								batch[i]->E.empty() ? nullptr : batch[i]->E.data()};
+	std::vector<uint32_t> O, D, E;
+	std::vector<uint64_t> voff, eoff;
+	clear_error();
+	int rc = build_union(csrs.data(), csrs.size(), O, D, E, voff, eoff);
+	if (!rc)
+	{
+		const nucleus34_csr u{voff.back(), eoff.back(), O.data(), D.data(), E.empty() ? nullptr : E.data()};
+		rc = upload(c, &u);
+	}
+	nucleus34_result r{};
+	if (!rc)
+	{
+		c.seg_eoff = eoff;
+		rc = run(c, NUCLEUS34_ONDEMAND, &r);
+	}
+	// results to the host: k of every request, triangle lists of those that ask
+	bool want_tris = false;
+	for (auto &q : batch)
+		want_tris = want_tris || (q->flags & NUCLEUS34_REQ_TRIANGLES);
+	std::vector<int32_t> K;
+	std::vector<uint32_t> tris;
+	if (!rc && c.T)
+	{
+		K.resize(c.T);
+		if (want_tris)
+			tris.resize(3 * c.T);
+		if (cudaMemcpyAsync(K.data(), c.dK, c.T * 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			(want_tris &&
+			 cudaMemcpyAsync(tris.data(), c.dtris, c.T * 12, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess) ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+			rc = fail(NUCLEUS34_E_CUDA, "serving: result copy");
+	}
+	const std::string err = rc ? std::string(nucleus34_last_error()) : std::string();
+	for (size_t i = 0; i < batch.size(); ++i)
+	{
+		Request &q = *batch[i];
+		q.status = rc;
+		q.error = err;
+		if (rc)
+			continue;
+		const uint64_t t0 = c.seg_toff[i], T = c.seg_toff[i + 1] - t0;
+		q.summary.triangle_count = T;
+		q.summary.four_clique_count = c.seg_q[i];
+		q.summary.k_max = c.seg_kmax[i];
+		q.summary.k_avg = T ? double(c.seg_ksum[i]) / double(T) : 0.0;
+		q.k.assign(K.begin() + t0, K.begin() + t0 + T);
+		if (q.flags & NUCLEUS34_REQ_TRIANGLES)
+		{
+			q.tris.assign(tris.begin() + 3 * t0, tris.begin() + 3 * (t0 + T));
+			const uint32_t eo = uint32_t(eoff[i]);
+			for (auto &x : q.tris)
+				x -= eo;
+		}
+	}
+	c.release_results();
+}
+
+// a request for its clique list: the direct variant, alone
+void serve_direct(Ctx &c, Request &q)
+{
+	clear_error();
+	const nucleus34_csr u{q.n, q.m, q.O.data(), q.D.data(), q.E.empty() ? nullptr : q.E.data()};
+	int rc = upload(c, &u);
+	nucleus34_result r{};
+	if (!rc)
+		rc = run(c, NUCLEUS34_DIRECT, &r);
+	if (!rc && c.T)
+	{
+		q.k.resize(c.T);
+		q.tris.resize(3 * c.T);
+		q.quds.resize(4 * c.Q);
+		if (cudaMemcpyAsync(q.k.data(), c.dK, c.T * 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaMemcpyAsync(q.tris.data(), c.dtris, c.T * 12, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			(c.Q && cudaMemcpyAsync(q.quds.data(), c.dquds, c.Q * 16, cudaMemcpyDeviceToHost, c.stream) !=
+						cudaSuccess) ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+			rc = fail(NUCLEUS34_E_CUDA, "serving: result copy");
+	}
+	q.status = rc;
+	q.error = rc ? std::string(nucleus34_last_error()) : std::string();
+	if (!rc)
+	{
+		q.summary.triangle_count = r.triangle_count;
+		q.summary.four_clique_count = r.four_clique_count;
+		q.summary.k_max = r.k_max;
+		q.summary.k_avg = r.k_avg;
+	}
+	c.release_results();
+}
+
+void worker_loop(nucleus34_server_s *s, size_t wi)
+{
+	Ctx &c = s->ctxs[wi]->c;
+	cudaSetDevice(c.device);
+	const uint64_t range_limit = 0xffffffffull / 3;
+	for (;;)
+	{
+		std::vector<std::shared_ptr<Request>> batch;
+		bool direct = false;
+		uint64_t take_bytes = 0;
+		{
+			std::unique_lock<std::mutex> lk(s->mu);
+			s->cv_work.wait(lk, [&] {
+				if (s->stop)
+					return true;
+				if (s->pending.empty())
+					return false;
+				// the head fits the memory left, or nothing else is running
+				const uint64_t free_b = s->budget > s->in_flight_bytes ? s->budget - s->in_flight_bytes : 0;
+				return s->pending.front()->est_bytes <= free_b || s->in_flight_bytes == 0;
+			});
+			if (s->stop && s->pending.empty())
+				return;
+			if (s->pending.empty())
+				continue;
+			uint64_t free_b = s->budget > s->in_flight_bytes ? s->budget - s->in_flight_bytes : 0;
+			// admission in arrival order: the head always (it fits, or runs
+			// alone on an idle device), then followers while they fit
+			auto head = s->pending.front();
+			direct = (head->flags & NUCLEUS34_REQ_CLIQUES) != 0;
+			batch.push_back(head);
+			s->pending.pop_front();
+			take_bytes = head->est_bytes;
+			uint64_t tri_bound = head->est_triangles;
+			if (!direct)
+			{
+				while (!s->pending.empty() && batch.size() < s->max_batch)
+				{
+					auto &q = s->pending.front();
+					if (q->flags & NUCLEUS34_REQ_CLIQUES)
+						break;
+					if (take_bytes + q->est_bytes > free_b || tri_bound + q->est_triangles > range_limit)
+						break;
+					take_bytes += q->est_bytes;
+					tri_bound += q->est_triangles;
+					batch.push_back(q);
+					s->pending.pop_front();
+				}
+			}
+			s->in_flight_bytes += take_bytes;
+			s->busy_workers++;
+			const auto now = clk::now();
+			for (auto &q : batch)
+				q->t_start = now;
+		}
+		if (direct)
+			serve_direct(c, *batch[0]);
+		else
+			serve_union(c, batch);
+		{
+			std::lock_guard<std::mutex> lk(s->mu);
+			s->in_flight_bytes -= take_bytes;
+			s->busy_workers--;
+			s->passes++;
+			const auto now = clk::now();
+			for (auto &q : batch)
+			{
+				q->done = true;
+				q->t_done = now;
+				q->pass = s->passes;
+				// the CSR copy is no longer needed
+				std::vector<uint32_t>().swap(q->O);
+				std::vector<uint32_t>().swap(q->D);
+				std::vector<uint32_t>().swap(q->E);
+			}
+			s->served += batch.size();
+		}
+		s->cv_done.notify_all();
+		s->cv_work.notify_all();
+	}
+}
+
+std::shared_ptr<Request> find(nucleus34_server s, uint64_t id)
+{
+	auto it = s->all.find(id);
+	return it == s->all.end() ? nullptr : it->second;
+}
+
+} // namespace
+
+extern "C" {
+
+int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_opts *sopts, nucleus34_server *out)
+{
+	if (!out)
+		return fail(NUCLEUS34_E_INVALID, "null argument");
+	*out = nullptr;
+	clear_error();
+	auto *s = new (std::nothrow) nucleus34_server_s();
+	if (!s)
+		return fail(NUCLEUS34_E_OOM_BUDGET, "host allocation failed");
+	if (opts)
+		s->opts = *opts;
+	const uint32_t nw = (sopts && sopts->workers) ? sopts->workers : 2u;
+	s->max_batch = (sopts && sopts->max_batch_graphs) ? sopts->max_batch_graphs : 256;
+	for (uint32_t i = 0; i < nw; ++i)
+	{
+		nucleus34_ctx ctx = nullptr;
+		int rc = create_ctx(opts, &ctx);
+		if (rc)
+		{
+			for (auto x : s->ctxs)
+				destroy_ctx(x);
+			delete s;
+			return rc;
+		}
+		s->ctxs.push_back(ctx);
+	}
+	// one budget shared by the passes in flight
+	s->budget = s->ctxs[0]->c.budget;
+	for (auto x : s->ctxs)
+		x->c.budget = s->budget;
+	for (uint32_t i = 0; i < nw; ++i)
+		s->workers.emplace_back(worker_loop, s, size_t(i));
+	*out = s;
+	return NUCLEUS34_OK;
+}
+
+int nucleus34_server_submit(nucleus34_server s, const nucleus34_csr *csr, uint32_t flags, uint64_t *id)
+{
+	if (!s || !csr || !id || (csr->n && !csr->D) || (csr->m && !csr->E))
+		return fail(NUCLEUS34_E_INVALID, "null argument");
+	clear_error();
+	auto q = std::make_shared<Request>();
+	q->flags = flags;
+	q->n = csr->n;
+	q->m = csr->m;
+	q->O.resize(csr->n + 1);
+	q->D.assign(csr->D, csr->D + csr->n);
+	q->E.assign(csr->E, csr->E + csr->m);
+	uint64_t acc = 0;
+	for (uint64_t u = 0; u < csr->n; ++u)
+	{
+		q->O[u] = uint32_t(acc);
+		acc += csr->D[u];
+	}
+	if (acc != csr->m)
+		return fail(NUCLEUS34_E_INVALID, "sum of D does not equal m");
+	q->O[csr->n] = uint32_t(acc);
+	const uint64_t w = wedge_bound(csr->D, csr->n);
+	q->est_triangles = w;
+	q->est_bytes = PASS_BYTES_PER_EDGE * csr->m +
+				   (flags & NUCLEUS34_REQ_CLIQUES ? DIRECT_BYTES_PER_WEDGE : PASS_BYTES_PER_TRIANGLE) * w;
+	q->t_submit = clk::now();
+	{
+		std::lock_guard<std::mutex> lk(s->mu);
+		q->id = s->next_id++;
+		s->all[q->id] = q;
+		s->pending.push_back(q);
+	}
+	*id = q->id;
+	s->cv_work.notify_one();
+	return NUCLEUS34_OK;
+}
+
+int nucleus34_server_wait(nucleus34_server s, uint64_t id, int64_t timeout_ms, nucleus34_request_info *info)
+{
+	if (!s)
+		return fail(NUCLEUS34_E_INVALID, "null server");
+	clear_error();
+	std::unique_lock<std::mutex> lk(s->mu);
+	auto q = find(s, id);
+	if (!q)
+		return fail(NUCLEUS34_E_INVALID, "unknown request id");
+	auto ready = [&] { return q->done; };
+	if (timeout_ms < 0)
+		s->cv_done.wait(lk, ready);
+	else if (!s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready))
+		return fail(NUCLEUS34_E_TIMEOUT, "request not finished within the timeout");
+	if (info)
+	{
+		nucleus34_request_info x{};
+		x.status = q->status;
+		x.summary = q->summary;
+		x.queue_seconds = std::chrono::duration<double>(q->t_start - q->t_submit).count();
+		x.latency_seconds = std::chrono::duration<double>(q->t_done - q->t_submit).count();
+		x.pass = q->pass;
+		x.direct = (q->flags & NUCLEUS34_REQ_CLIQUES) ? 1 : 0;
+		*info = x;
+	}
+	if (q->status)
+		return fail(q->status, q->error);
+	return NUCLEUS34_OK;
+}
+
+int nucleus34_server_copy_k(nucleus34_server s, uint64_t id, int32_t *k_out, uint32_t *tris_out)
+{
+	if (!s)
+		return fail(NUCLEUS34_E_INVALID, "null server");
+	std::lock_guard<std::mutex> lk(s->mu);
+	auto q = find(s, id);
+	if (!q || !q->done)
+		return fail(NUCLEUS34_E_STATE, "request unknown or not finished");
+	if (q->status)
+		return fail(q->status, q->error);
+	if (k_out && !q->k.empty())
+		std::copy(q->k.begin(), q->k.end(), k_out);
+	if (tris_out)
+	{
+		if (q->tris.size() != 3 * q->summary.triangle_count)
+			return fail(NUCLEUS34_E_STATE, "the request did not ask for its triangle list");
+		std::copy(q->tris.begin(), q->tris.end(), tris_out);
+	}
+	return NUCLEUS34_OK;
+}
+
+int nucleus34_server_copy_quds(nucleus34_server s, uint64_t id, uint64_t first, uint64_t count, uint32_t *quds_out)
+{
+	if (!s || (count && !quds_out))
+		return fail(NUCLEUS34_E_INVALID, "null argument");
+	std::lock_guard<std::mutex> lk(s->mu);
+	auto q = find(s, id);
+	if (!q || !q->done)
+		return fail(NUCLEUS34_E_STATE, "request unknown or not finished");
+	if (!(q->flags & NUCLEUS34_REQ_CLIQUES))
+		return fail(NUCLEUS34_E_STATE, "the request did not ask for its four-clique list");
+	const uint64_t Q = q->quds.size() / 4;
+	if (first > Q || count > Q - first)
+		return fail(NUCLEUS34_E_INVALID, "clique range out of bounds");
+	std::copy(q->quds.begin() + 4 * first, q->quds.begin() + 4 * (first + count), quds_out);
+	return NUCLEUS34_OK;
+}
+
+int nucleus34_server_release(nucleus34_server s, uint64_t id)
+{
+	if (!s)
+		return fail(NUCLEUS34_E_INVALID, "null server");
+	std::lock_guard<std::mutex> lk(s->mu);
+	auto it = s->all.find(id);
+	if (it == s->all.end() || !it->second->done)
+		return fail(NUCLEUS34_E_STATE, "request unknown or not finished");
+	s->all.erase(it);
+	return NUCLEUS34_OK;
+}
+
+int nucleus34_server_stats(nucleus34_server s, nucleus34_server_counters *out)
+{
+	if (!s || !out)
+		return fail(NUCLEUS34_E_INVALID, "null argument");
+	std::lock_guard<std::mutex> lk(s->mu);
+	nucleus34_server_counters x{};
+	x.passes = s->passes;
+	x.served = s->served;
+	x.pending = s->pending.size();
+	x.busy_workers = s->busy_workers;
+	x.workers = s->workers.size();
+	x.in_flight_bytes = s->in_flight_bytes;
+	x.budget_bytes = s->budget;
+	*out = x;
+	return NUCLEUS34_OK;
+}
+
+void nucleus34_server_destroy(nucleus34_server s)
+{
+	if (!s)
+		return;
+	{
+		std::lock_guard<std::mutex> lk(s->mu);
+		s->stop = true;
+	}
+	s->cv_work.notify_all();
+	for (auto &t : s->workers)
+		t.join();
+	for (auto x : s->ctxs)
+		destroy_ctx(x);
+	delete s;
+}
+
+} // extern "C"

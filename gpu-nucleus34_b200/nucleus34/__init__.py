@@ -46,6 +46,8 @@ EXPORTED = (
     "nucleus34_decompose", "nucleus34_decompose_ondemand", "nucleus34_copy_k",
     "nucleus34_copy_quds", "nucleus34_write_kfile", "nucleus34_free", "nucleus34_release_cached_memory",
     "nucleus34_batch_decompose", "nucleus34_batch_summary", "nucleus34_batch_copy_k", "nucleus34_batch_free",
+    "nucleus34_server_create", "nucleus34_server_submit", "nucleus34_server_wait", "nucleus34_server_copy_k",
+    "nucleus34_server_copy_quds", "nucleus34_server_release", "nucleus34_server_stats", "nucleus34_server_destroy",
     "nucleus34_strerror", "nucleus34_last_error",
     "nucleus34_ctx_create", "nucleus34_ctx_upload", "nucleus34_ctx_run",
     "nucleus34_ctx_copy_k", "nucleus34_ctx_destroy", "nucleus34_ctx_verify",
@@ -109,6 +111,27 @@ class GraphSummary(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("workers", C.c_uint32), ("max_batch_graphs", C.c_uint64)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("summary", GraphSummary), ("queue_seconds", C.c_double),
+                ("latency_seconds", C.c_double), ("pass_", C.c_uint64), ("direct", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {"status": self.status, **self.summary.as_dict(), "queue_seconds": self.queue_seconds,
+                "latency_seconds": self.latency_seconds, "pass": self.pass_, "direct": bool(self.direct)}
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("passes", "served", "pending", "busy_workers", "workers",
+                                          "in_flight_bytes", "budget_bytes")]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class Graph(C.Structure):
     _fields_ = [("n", C.c_uint64), ("m", C.c_uint64), ("O", C.POINTER(C.c_uint32)),
                 ("D", C.POINTER(C.c_uint32)), ("E", C.POINTER(C.c_uint32))]
@@ -159,6 +182,22 @@ def lib() -> C.CDLL:
     L.nucleus34_batch_copy_k.restype = C.c_int
     L.nucleus34_batch_free.argtypes = [C.c_void_p]
     L.nucleus34_batch_free.restype = None
+    L.nucleus34_server_create.argtypes = [C.POINTER(Opts), C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]
+    L.nucleus34_server_create.restype = C.c_int
+    L.nucleus34_server_submit.argtypes = [C.c_void_p, C.POINTER(Csr), C.c_uint32, C.POINTER(C.c_uint64)]
+    L.nucleus34_server_submit.restype = C.c_int
+    L.nucleus34_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int64, C.POINTER(RequestInfo)]
+    L.nucleus34_server_wait.restype = C.c_int
+    L.nucleus34_server_copy_k.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_int32), u32p]
+    L.nucleus34_server_copy_k.restype = C.c_int
+    L.nucleus34_server_copy_quds.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_uint64, u32p]
+    L.nucleus34_server_copy_quds.restype = C.c_int
+    L.nucleus34_server_release.argtypes = [C.c_void_p, C.c_uint64]
+    L.nucleus34_server_release.restype = C.c_int
+    L.nucleus34_server_stats.argtypes = [C.c_void_p, C.POINTER(ServerCounters)]
+    L.nucleus34_server_stats.restype = C.c_int
+    L.nucleus34_server_destroy.argtypes = [C.c_void_p]
+    L.nucleus34_server_destroy.restype = None
     L.nucleus34_ctx_create.argtypes = [C.POINTER(Opts), C.POINTER(C.c_void_p)]
     L.nucleus34_ctx_create.restype = C.c_int
     L.nucleus34_ctx_upload.argtypes = [C.c_void_p, C.POINTER(Csr)]
@@ -396,6 +435,71 @@ def batch_decompose(graphs, device: int = 0, mem_budget_bytes: int = 0, flags: i
     h = C.c_void_p()
     _check(L.nucleus34_batch_decompose(arr, len(graphs), C.byref(opts), C.byref(res), C.byref(h)), "batch_decompose")
     return Batch(h, res.as_dict(), len(graphs))
+
+
+REQ_CLIQUES = 0x1
+REQ_TRIANGLES = 0x2
+
+
+class Server:
+    """nucleus34_server_*: continuous batching of decomposition requests."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0, workers: int = 2, max_batch_graphs: int = 256,
+                 flags: int = 0):
+        self._L = lib()
+        opts = make_opts(device, mem_budget_bytes, flags=flags)
+        so = ServerOpts(workers, max_batch_graphs)
+        self._h = C.c_void_p()
+        _check(self._L.nucleus34_server_create(C.byref(opts), C.byref(so), C.byref(self._h)), "server_create")
+
+    def submit(self, g: HostGraph, cliques: bool = False, triangles: bool = False) -> int:
+        rid = C.c_uint64()
+        csr = g.csr()
+        flags = (REQ_CLIQUES if cliques else 0) | (REQ_TRIANGLES if triangles else 0)
+        _check(self._L.nucleus34_server_submit(self._h, C.byref(csr), flags, C.byref(rid)), "server_submit")
+        return int(rid.value)
+
+    def wait(self, rid: int, timeout_ms: int = -1) -> dict:
+        info = RequestInfo()
+        _check(self._L.nucleus34_server_wait(self._h, rid, timeout_ms, C.byref(info)), "server_wait")
+        return info.as_dict()
+
+    def copy_k(self, rid: int, T: int, with_tris: bool = False):
+        k = np.zeros(T, np.int32)
+        tris = np.zeros(3 * T, np.uint32) if with_tris else None
+        _check(self._L.nucleus34_server_copy_k(self._h, rid, k.ctypes.data_as(C.POINTER(C.c_int32)),
+                                               _u32p(tris) if tris is not None else None), "server_copy_k")
+        return (k, tris.reshape(-1, 3)) if with_tris else k
+
+    def copy_quds(self, rid: int, first: int, count: int) -> np.ndarray:
+        q = np.zeros(4 * count, np.uint32)
+        _check(self._L.nucleus34_server_copy_quds(self._h, rid, first, count, _u32p(q)), "server_copy_quds")
+        return q.reshape(-1, 4)
+
+    def release(self, rid: int) -> None:
+        _check(self._L.nucleus34_server_release(self._h, rid), "server_release")
+
+    def stats(self) -> dict:
+        c = ServerCounters()
+        _check(self._L.nucleus34_server_stats(self._h, C.byref(c)), "server_stats")
+        return c.as_dict()
+
+    def close(self) -> None:
+        if self._h:
+            self._L.nucleus34_server_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Context:

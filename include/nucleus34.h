@@ -219,6 +219,57 @@ int nucleus34_batch_summary(nucleus34_batch b, uint64_t index, nucleus34_graph_s
 int nucleus34_batch_copy_k(nucleus34_batch b, uint64_t index, int32_t *k_out, uint32_t *tris_out);
 void nucleus34_batch_free(nucleus34_batch b);
 
+/* ---- serving: continuous batching of decomposition requests -------------- */
+
+/* A request loop with device-resident state. Workers (one context and stream
+ * each) admit pending requests in arrival order while their estimated memory
+ * fits what the budget (opts.mem_budget_bytes) has left, decompose them in one
+ * union pass, and copy each request's results to the host. Requests that
+ * arrive while passes run join the next pass; passes of different workers
+ * overlap on the device. Requests flagged NUCLEUS34_REQ_CLIQUES are routed to
+ * the direct variant (their four-clique list is kept) and run alone; all
+ * others run on-demand. A request's results equal those of the graph
+ * decomposed alone. No reference counterpart. */
+typedef struct nucleus34_server_s *nucleus34_server;
+
+#define NUCLEUS34_REQ_CLIQUES 0x1u   /* direct variant: keep the four-clique list */
+#define NUCLEUS34_REQ_TRIANGLES 0x2u /* keep the triangle list (k alone otherwise) */
+
+typedef struct
+{
+	uint32_t workers;             /* concurrent passes, 0 = 2 */
+	uint64_t max_batch_graphs;    /* requests per pass, 0 = 256 */
+} nucleus34_server_opts;
+
+typedef struct
+{
+	int status;                   /* the request's own result code */
+	nucleus34_graph_summary summary;
+	double queue_seconds;         /* submit -> admitted to a pass */
+	double latency_seconds;       /* submit -> results on the host */
+	uint64_t pass;                /* sequence number of the pass that served it */
+	int direct;                   /* 1 if routed to the direct variant */
+} nucleus34_request_info;
+
+typedef struct
+{
+	uint64_t passes, served, pending, busy_workers, workers, in_flight_bytes, budget_bytes;
+} nucleus34_server_counters;
+
+int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_opts *sopts, nucleus34_server *out);
+/* Copies the CSR and queues it; returns at once with the request id. */
+int nucleus34_server_submit(nucleus34_server s, const nucleus34_csr *csr, uint32_t flags, uint64_t *id);
+/* Waits for request id (timeout_ms < 0: without limit; NUCLEUS34_E_TIMEOUT when
+ * it runs out); returns the request's own status and fills info. */
+int nucleus34_server_wait(nucleus34_server s, uint64_t id, int64_t timeout_ms, nucleus34_request_info *info);
+int nucleus34_server_copy_k(nucleus34_server s, uint64_t id, int32_t *k_out, uint32_t *tris_out);
+int nucleus34_server_copy_quds(nucleus34_server s, uint64_t id, uint64_t first, uint64_t count, uint32_t *quds_out);
+/* Forgets a finished request and its host results. */
+int nucleus34_server_release(nucleus34_server s, uint64_t id);
+int nucleus34_server_stats(nucleus34_server s, nucleus34_server_counters *out);
+/* Finishes the queued requests, then stops the workers. */
+void nucleus34_server_destroy(nucleus34_server s);
+
 /* ---- triangle listing without allocation --------------------------------- */
 
 /* No counterpart in the reference. For callers that cannot allocate device
