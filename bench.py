@@ -64,6 +64,10 @@ def parse():
     p.add_argument("--workload", default="decompose", choices=["decompose", "batch", "serve"],
                    help="decompose: the headline single-graph metric; batch: the batched form "
                         "(graphs/s of nucleus34_batch_decompose vs one decomposition per graph)")
+    p.add_argument("--capture-run", action="store_true",
+                   help="exactly one decomposition of the workload graph (for ncu captures); prints its record")
+    p.add_argument("--peel-profile", action="store_true",
+                   help="with --capture-run: per-step profiling mode (plain launches, per-round trace on stderr)")
     p.add_argument("--batch-graphs", type=int, default=4096)
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-max-edges", type=float, default=1e6)
@@ -366,8 +370,23 @@ def run_serve(a):
     return 0 if mism == 0 else 1
 
 
+def capture_run(a):
+    """One decomposition and nothing else, so that ncu launch indices are
+    those of that decomposition alone."""
+    import nucleus34 as n34
+    g = make_graph(n34, a.scale, a.edge_factor, a.seed)
+    flags = n34.OPT_PROFILE_PEEL if a.peel_profile else 0
+    with n34.Context(flags=flags) as ctx:
+        ctx.upload(g)
+        r = ctx.run(a.variant)
+    print(json.dumps({"workload": workload_name(a), **r}), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if a.capture_run:
+        return capture_run(a)
     if a.workload == "batch":
         return run_batch(a)
     if a.workload == "serve":
@@ -531,10 +550,11 @@ def main():
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
-# byte, from ncu captures of a smaller case of the same workload (R-MAT scale
-# 17; profiles/), applied to this run's algorithmic bytes: the traffic of both
+# byte, from one ncu capture of a smaller case of the same workload (R-MAT
+# scale 17: the whole peel, whose traffic the debit dominates, and the support
+# launch), applied to this run's algorithmic bytes: the traffic of both
 # kernels grows with the lists they read.
-NCU_TRAFFIC_PER_ALG_BYTE = {"debit": None, "k_support": None}
+NCU_TRAFFIC_PER_ALG_BYTE = {"debit": 1.018, "k_support": 0.028}
 
 
 def roofline(r, prof, peaks, kind):

@@ -15,8 +15,8 @@
 // once, instead of a launch sequence per graph. Per-graph counts and k
 // statistics come from segment reductions over the shared arrays.
 //
-// The reference has no batched form; this implements the batch row of the
-// design's next steps with the reference's per-graph semantics unchanged.
+// The reference has no batched form (one graph per process); every graph's
+// results keep the reference's per-graph semantics.
 #include "pipeline.cuh"
 
 #include <algorithm>

@@ -15,7 +15,7 @@ def declared_functions():
     return sorted(set(re.findall(r"\b(nucleus34_[a-z0-9_]+)\s*\(", text)))
 
 
-def test_header_declares_the_north_star_entry_points():
+def test_header_declares_the_drop_in_entry_points():
     names = declared_functions()
     for fn in ("nucleus34_decompose", "nucleus34_decompose_ondemand", "nucleus34_copy_k",
                "nucleus34_free", "nucleus34_strerror"):
