@@ -51,6 +51,9 @@ struct CtlX
 	unsigned long long peeled_at_compact;
 	unsigned long long live_at_compact;
 	uint32_t compactions;
+	// profiling counters of k_debit_flags_warp (filled only when stats is set)
+	uint32_t stats;
+	unsigned long long st_tri, st_merge_entries, st_steps, st_lookups, st_resolves, st_staged, st_found;
 };
 
 __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
@@ -70,6 +73,8 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
 		ctl->peeled_at_compact = 0;
 		ctl->live_at_compact = T;
 		ctl->compactions = 0;
+		ctl->st_tri = ctl->st_merge_entries = ctl->st_steps = ctl->st_lookups = 0;
+		ctl->st_resolves = ctl->st_staged = ctl->st_found = 0;
 	}
 }
 
@@ -566,6 +571,14 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 #ifndef N34_L2_PREFETCH
 #define N34_L2_PREFETCH 1
 #endif
+#ifndef N34_C_STAGE
+#define N34_C_STAGE 768
+#endif
+// Work counters of the warp debit in profiling runs (a diagnostic build
+// option: the counters cost registers in the hot loop).
+#ifndef N34_PEEL_STATS
+#define N34_PEEL_STATS 0
+#endif
 #ifndef N34_DEBIT_MINB
 #define N34_DEBIT_MINB 6
 #endif
@@ -576,6 +589,9 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 {
 	constexpr int WARPS = PEEL_THREADS / 32;
 	__shared__ uint32_t qx[WARPS][64], qp0[WARPS][64], qp1[WARPS][64];
+#if N34_C_STAGE > 0
+	__shared__ uint32_t cstage_all[WARPS][N34_C_STAGE];
+#endif
 	if (ctl->c.done)
 		return;
 	const uint32_t nF = ctl->c.nF;
@@ -603,25 +619,91 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 			prefetch_range_l2(itri, L.b0, L.b1);
 		}
 #endif
+#if N34_PEEL_STATS
+		const bool st = ctl->stats != 0;
+#else
+		constexpr bool st = false;
+#endif
+		unsigned long long n_steps = 0, n_lookups = 0, n_resolves = 0, n_staged = 0, n_found = 0;
 		uint32_t lo_c = L.c0;
 		uint32_t queued = 0; // warp-uniform
-		// one sample of C serves every resolve of this triangle
-		const WarpSample cs = warp_sample(third, L.c0, L.c1);
+		// How the lookups on C are served, decided at the first resolve
+		// (warp-uniform): 0 undecided, 1 from a copy of C's thirds staged in
+		// shared memory (C short against the lookups: one coalesced read of
+		// C instead of a search path per lookup), 2 by sampled binary
+		// searches in global memory (one sample of C per triangle).
+		uint32_t mode = 0, stage_base = 0, stage_len = 0;
+		WarpSample cs{0u, 0u, false};
+#if N34_C_STAGE > 0
+		uint32_t *cstage = cstage_all[wib];
+#endif
 		// resolves the first n (<= 32) queued entries; called by all lanes
 		auto resolve = [&](uint32_t n) {
 			__syncwarp();
+			if (mode == 0)
+			{
+				const uint32_t len = L.c1 - lo_c;
+#if N34_C_STAGE > 0
+				if (len <= N34_C_STAGE && len <= 32u * n)
+				{
+					for (uint32_t i = lane; i < len; i += 32)
+						cstage[i] = __ldg(third + lo_c + i);
+					__syncwarp();
+					stage_base = lo_c;
+					stage_len = len;
+					mode = 1;
+				}
+				else
+#endif
+				{
+					cs = warp_sample(third, lo_c, L.c1);
+					mode = 2;
+				}
+			}
 			const bool v = lane < n;
 			const uint32_t x = v ? bx[lane] : 0xffffffffu;
 			const uint32_t q0 = v ? b0[lane] : DEAD, q1 = v ? b1[lane] : DEAD;
-			const uint32_t pc = sampled_lower_bound(third, cs, lo_c, L.c1, v, x);
-			lo_c = __shfl_sync(FULL, pc, n - 1); // thirds ascend through the queue
-			bool hit[3] = {false, false, false};
-			uint32_t q2 = DEAD, xc = 0xffffffffu;
-			if (v && pc < L.c1)
+			uint32_t pc = L.c1, xc = 0xffffffffu, q2 = DEAD;
+#if N34_C_STAGE > 0
+			if (mode == 1)
 			{
-				xc = __ldg(third + pc);
-				q2 = __ldg(itri + pc);
+				if (v)
+				{
+					// lower bound of x in the staged thirds from lo_c on
+					uint32_t lo = lo_c - stage_base, cnt = stage_len - lo;
+					while (cnt > 0)
+					{
+						const uint32_t half = cnt >> 1;
+						const bool less = cstage[lo + half] < x;
+						lo = less ? lo + half + 1 : lo;
+						cnt = less ? cnt - half - 1 : half;
+					}
+					pc = stage_base + lo;
+					if (lo < stage_len)
+						xc = cstage[lo];
+					if (xc == x)
+						q2 = __ldg(itri + pc);
+				}
 			}
+			else
+#endif
+			{
+				pc = sampled_lower_bound(third, cs, lo_c, L.c1, v, x);
+				if (v && pc < L.c1)
+				{
+					xc = __ldg(third + pc);
+					q2 = __ldg(itri + pc);
+				}
+			}
+			lo_c = __shfl_sync(FULL, pc, n - 1); // thirds ascend through the queue
+			if (st)
+			{
+				n_lookups += n;
+				n_resolves += 1;
+				n_staged += mode == 1;
+				n_found += __popc(__ballot_sync(FULL, v && xc == x));
+			}
+			bool hit[3] = {false, false, false};
 			// absent from C: that partner died and was compacted away (clique destroyed)
 			if (v && xc == x && !(q2 & DEAD))
 				settle_flags(t, q0, q1, q2, S, level, hit);
@@ -642,6 +724,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 		};
 		warp_intersect2<true>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
 												  uint32_t qb) {
+			n_steps += st;
 			// a clique is looked up on C only if its partners on A and B are
 			// alive and neither is a dying triangle of smaller id (its owner)
 			const bool live = found && !(qa & DEAD) && !(qb & DEAD) &&
@@ -682,6 +765,16 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 		if (queued)
 			resolve(queued);
 		__syncwarp();
+		if (st && lane == 0)
+		{
+			atomicAdd(&ctl->st_tri, 1ull);
+			atomicAdd(&ctl->st_merge_entries, (unsigned long long)(L.a1 - L.a0 + L.b1 - L.b0));
+			atomicAdd(&ctl->st_steps, n_steps);
+			atomicAdd(&ctl->st_lookups, n_lookups);
+			atomicAdd(&ctl->st_resolves, n_resolves);
+			atomicAdd(&ctl->st_staged, n_staged);
+			atomicAdd(&ctl->st_found, n_found);
+		}
 	}
 }
 
@@ -1048,6 +1141,14 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		const uint32_t gwarp = grid_for(c, T, PEEL_THREADS / 32, 16);
 		k_peel_init<<<gscan, PEEL_THREADS, 0, c.stream>>>(K, T, ctl);
 		c.launches++;
+		{
+			const uint32_t on = (c.opt_flags & NUCLEUS34_OPT_PROFILE_PEEL) ? 1u : 0u;
+			if (cudaMemcpyAsync(&ctl->stats, &on, 4, cudaMemcpyHostToDevice, c.stream) != cudaSuccess)
+			{
+				rc = fail(NUCLEUS34_E_CUDA, "peel control");
+				break;
+			}
+		}
 		// Profiling (NUCLEUS34_OPT_PROFILE_PEEL): rounds run as plain launches
 		// with an event after every step; per-step totals go to stderr.
 		const bool profile = (c.opt_flags & NUCLEUS34_OPT_PROFILE_PEEL) != 0;
@@ -1253,9 +1354,16 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			cudaFreeHost(trace_buf);
 		if (profile)
 		{
-			uint32_t compactions = 0;
-			cudaMemcpy(&compactions, &ctl->compactions, 4, cudaMemcpyDeviceToHost);
-			std::fprintf(stderr, "[peel-profile] rounds=%llu compactions=%u", (unsigned long long)rounds, compactions);
+			CtlX hx{};
+			cudaMemcpy(&hx, ctl, sizeof(CtlX), cudaMemcpyDeviceToHost);
+			if (N34_PEEL_STATS)
+				std::fprintf(stderr,
+						 "[peel-counters] warp-debit triangles=%llu merged_entries=%llu merge_steps=%llu lookups=%llu "
+						 "resolves=%llu staged_resolves=%llu found_on_c=%llu\n",
+						 hx.st_tri, hx.st_merge_entries, hx.st_steps, hx.st_lookups, hx.st_resolves, hx.st_staged,
+						 hx.st_found);
+			std::fprintf(stderr, "[peel-profile] rounds=%llu compactions=%u", (unsigned long long)rounds,
+						 hx.compactions);
 			for (int j = 0; j < PROF_STEPS; ++j)
 				std::fprintf(stderr, " %s=%.1fms", prof_names[j], prof_ms[j]);
 			std::fprintf(stderr, "\n");
