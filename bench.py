@@ -554,7 +554,7 @@ def main():
 # scale 17: the whole peel, whose traffic the debit dominates, and the support
 # launch), applied to this run's algorithmic bytes: the traffic of both
 # kernels grows with the lists they read.
-NCU_TRAFFIC_PER_ALG_BYTE = {"debit": 1.018, "k_support": 0.028}
+NCU_TRAFFIC_PER_ALG_BYTE = {"debit": 1.007, "k_support": 0.028}
 
 
 def roofline(r, prof, peaks, kind):
