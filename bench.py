@@ -383,6 +383,22 @@ def capture_run(a):
     return 0
 
 
+def max_over_ranks(x: float, device: str) -> float:
+    """The slowest rank's time (all_reduce MAX over the process group): the
+    job is done when its last replica is."""
+    import torch
+    import torch.distributed as tdist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    tdist.all_reduce(t, op=tdist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world: int, triangles: int, steps: int, seconds: float) -> float:
+    """Whole-job throughput of N replicas: every rank peels the workload's
+    triangles once per step, all within the slowest rank's time."""
+    return world * triangles * steps / seconds
+
+
 def main():
     a = parse()
     if a.capture_run:
@@ -455,11 +471,9 @@ def main():
     T = results[-1]["triangle_count"]
     dev_time = sum(times)
     if dist:
-        tt = torch.tensor([dev_time], dtype=torch.float64, device=f"cuda:{device}")
-        tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
-        dev_time = float(tt.item())
+        dev_time = max_over_ranks(dev_time, f"cuda:{device}")
     ms_per_step = dev_time / a.steps * 1e3
-    value = world * T * a.steps / dev_time
+    value = job_value(world, T, a.steps, dev_time)
     launches = sum(r["gpu_launches"] for r in results)
     ctx.close()
 
@@ -504,10 +518,8 @@ def main():
             e2e_times.append(t1 - t0)
         et = sum(e2e_times)
         if dist:
-            tt = torch.tensor([et], dtype=torch.float64, device=f"cuda:{device}")
-            tdist.all_reduce(tt, op=tdist.ReduceOp.MAX)
-            et = float(tt.item())
-        e2e = {"value": world * T * len(e2e_times) / et, "unit": UNIT,
+            et = max_over_ranks(et, f"cuda:{device}")
+        e2e = {"value": job_value(world, T, len(e2e_times), et), "unit": UNIT,
                "h2d_bytes_per_step": int(4 * (2 * g.n + g.m)), "d2h_bytes_per_step": int(4 * T),
                "ms_per_step": et / len(e2e_times) * 1e3,
                "api": "nucleus34_decompose_ondemand + nucleus34_copy_k" if a.variant == "ondemand"
