@@ -152,7 +152,9 @@ void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch)
 				x -= eo;
 		}
 	}
+	// a finished pass holds nothing on the device (admission counts on it)
 	c.release_results();
+	c.release_graph();
 }
 
 // a request for its clique list: the direct variant, alone
@@ -185,7 +187,9 @@ void serve_direct(Ctx &c, Request &q)
 		q.summary.k_max = r.k_max;
 		q.summary.k_avg = r.k_avg;
 	}
+	// a finished pass holds nothing on the device (admission counts on it)
 	c.release_results();
+	c.release_graph();
 }
 
 void worker_loop(nucleus34_server_s *s, size_t wi)
@@ -321,6 +325,8 @@ int nucleus34_server_submit(nucleus34_server s, const nucleus34_csr *csr, uint32
 	if (!s || !csr || !id || (csr->n && !csr->D) || (csr->m && !csr->E))
 		return fail(NUCLEUS34_E_INVALID, "null argument");
 	clear_error();
+	if (csr->m > 0xffffffffull || csr->n >= 0xffffffffull)
+		return fail(NUCLEUS34_E_RANGE32, "graph exceeds 32-bit vertex/edge ids");
 	auto q = std::make_shared<Request>();
 	q->flags = flags;
 	q->n = csr->n;
