@@ -886,3 +886,177 @@ int oracle_decompose(const oracle_graph *g, uint64_t quds_cap, oracle_result *r)
 	free_incidence(&inc);
 	return OR_OK;
 }
+
+/* ------------------------------------------------------------------------- */
+/* level-synchronous peel with death rounds, and the result certificate      */
+/* (checker side; no counterpart in the reference)                           */
+/* ------------------------------------------------------------------------- */
+
+/* The device peel's rules, restated on one thread: rounds at a level; a
+ * round's frontier dies together; a clique belongs to its first member to
+ * die, ties to the lowest id, and its owner debits the members still alive;
+ * a triangle whose support reaches the level joins the next round; an empty
+ * frontier moves the level to level+1 if some support is there, else to the
+ * minimum support. Gives the same k as the bucket peel (the numbers are
+ * unique) plus each triangle's death round. */
+typedef struct
+{
+	const uint8_t *state; /* 0 alive, 1 dying this round, 2 dead */
+	int32_t *S;
+	int64_t level;
+	uint32_t t;
+	uint32_t *next;
+	uint64_t nnext;
+} round_ctx;
+
+static void round_clique(void *vctx, uint32_t x, uint32_t p1, uint32_t p2, uint32_t p3)
+{
+	(void)x;
+	round_ctx *c = vctx;
+	const uint32_t m[3] = {p1, p2, p3};
+	for (int s = 0; s < 3; ++s)
+	{
+		if (c->state[m[s]] == 2)
+			return; /* destroyed in an earlier round */
+		if (c->state[m[s]] == 1 && m[s] < c->t)
+			return; /* owned by a lower dying member */
+	}
+	for (int s = 0; s < 3; ++s)
+		if (c->state[m[s]] == 0 && --c->S[m[s]] == c->level)
+			c->next[c->nnext++] = m[s];
+}
+
+int oracle_peel_rounds(const oracle_graph *g, const uint32_t *tris, uint64_t T, int32_t *k, uint32_t *rounds)
+{
+	if (T == 0)
+		return OR_OK;
+	incidence inc;
+	int rc = build_incidence(g, tris, T, &inc);
+	if (rc)
+		return rc;
+	int32_t *S = malloc(T * sizeof(int32_t));
+	uint8_t *state = calloc(T, 1);
+	uint32_t *front = malloc(T * sizeof(uint32_t)), *next = malloc(T * sizeof(uint32_t));
+	if (!S || !state || !front || !next)
+	{
+		free(S), free(state), free(front), free(next);
+		free_incidence(&inc);
+		return OR_ENOMEM;
+	}
+	for (uint64_t t = 0; t < T; ++t)
+		S[t] = (int32_t)for_each_clique(&inc, tris + 3 * t, NULL, NULL);
+	int64_t level = -1;
+	uint32_t round = 0;
+	uint64_t nf = 0, peeled = 0;
+	while (peeled < T)
+	{
+		if (nf == 0)
+		{
+			/* level change */
+			int64_t mn = INT64_MAX;
+			for (uint64_t t = 0; t < T; ++t)
+				if (state[t] == 0 && S[t] < mn)
+					mn = S[t];
+			level = mn <= level + 1 ? level + 1 : mn;
+			for (uint64_t t = 0; t < T; ++t)
+				if (state[t] == 0 && S[t] <= level)
+					front[nf++] = (uint32_t)t;
+		}
+		for (uint64_t i = 0; i < nf; ++i)
+		{
+			k[front[i]] = (int32_t)level;
+			rounds[front[i]] = round;
+			state[front[i]] = 1;
+		}
+		round_ctx rc2 = {state, S, level, 0, next, 0};
+		for (uint64_t i = 0; i < nf; ++i)
+		{
+			rc2.t = front[i];
+			for_each_clique(&inc, tris + 3 * (uint64_t)front[i], round_clique, &rc2);
+		}
+		for (uint64_t i = 0; i < nf; ++i)
+			state[front[i]] = 2;
+		peeled += nf;
+		memcpy(front, next, rc2.nnext * sizeof(uint32_t));
+		nf = rc2.nnext;
+		++round;
+	}
+	free(S), free(state), free(front), free(next);
+	free_incidence(&inc);
+	return OR_OK;
+}
+
+/* Certificate of a peel result, the conditions the device check applies:
+ * (A) t has at least k(t) cliques whose other triangles all have k >= k(t);
+ * (B) t has at most k(t) cliques whose other triangles died in round r(t) or
+ *     later (its support when its round began);
+ * (C) the triangles of a round share one level, non-decreasing over rounds.
+ * Returns the number of failing triangles plus failing rounds, or a negative
+ * error code. */
+typedef struct
+{
+	const int32_t *k;
+	const uint32_t *r;
+	int32_t kt;
+	uint32_t rt;
+	uint32_t a, b;
+} cert_ctx;
+
+static void cert_clique(void *vctx, uint32_t x, uint32_t p1, uint32_t p2, uint32_t p3)
+{
+	(void)x;
+	cert_ctx *c = vctx;
+	if (c->k[p1] >= c->kt && c->k[p2] >= c->kt && c->k[p3] >= c->kt)
+		c->a++;
+	if (c->r[p1] >= c->rt && c->r[p2] >= c->rt && c->r[p3] >= c->rt)
+		c->b++;
+}
+
+int64_t oracle_certify(const oracle_graph *g, const uint32_t *tris, uint64_t T, const int32_t *k,
+					   const uint32_t *rounds)
+{
+	if (T == 0)
+		return 0;
+	incidence inc;
+	int rc = build_incidence(g, tris, T, &inc);
+	if (rc)
+		return rc;
+	int64_t bad = 0;
+	uint32_t rmax = 0;
+	for (uint64_t t = 0; t < T; ++t)
+	{
+		cert_ctx c = {k, rounds, k[t], rounds[t], 0, 0};
+		for_each_clique(&inc, tris + 3 * t, cert_clique, &c);
+		if (k[t] < 0 || (int64_t)c.a < k[t] || (int64_t)c.b > k[t])
+			++bad;
+		if (rounds[t] > rmax)
+			rmax = rounds[t];
+	}
+	free_incidence(&inc);
+	int32_t *lo = malloc(((uint64_t)rmax + 1) * sizeof(int32_t)), *hi = malloc(((uint64_t)rmax + 1) * sizeof(int32_t));
+	if (!lo || !hi)
+	{
+		free(lo), free(hi);
+		return OR_ENOMEM;
+	}
+	for (uint64_t r = 0; r <= rmax; ++r)
+		lo[r] = INT32_MAX, hi[r] = -1;
+	for (uint64_t t = 0; t < T; ++t)
+	{
+		if (k[t] < lo[rounds[t]])
+			lo[rounds[t]] = k[t];
+		if (k[t] > hi[rounds[t]])
+			hi[rounds[t]] = k[t];
+	}
+	int32_t prev = -1;
+	for (uint64_t r = 0; r <= rmax; ++r)
+	{
+		if (hi[r] < 0)
+			continue;
+		if (lo[r] != hi[r] || lo[r] < prev)
+			++bad;
+		prev = hi[r];
+	}
+	free(lo), free(hi);
+	return bad;
+}

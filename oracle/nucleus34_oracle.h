@@ -63,6 +63,13 @@ void oracle_result_free(oracle_result *r);
 uint64_t oracle_count_triangles(const oracle_graph *g);
 /* four-cliques counted by oriented neighbourhoods (independent of the incidence) */
 uint64_t oracle_count_k4(const oracle_graph *g);
+/* Level-synchronous peel (the device peel's rules) on the canonical triangle
+ * list tris (3T): k and each triangle's death round. */
+int oracle_peel_rounds(const oracle_graph *g, const uint32_t *tris, uint64_t T, int32_t *k, uint32_t *rounds);
+/* Certificate check of (k, rounds): number of failing triangles and rounds
+ * (0: k are exactly the (3,4)-nucleus numbers), or a negative error code. */
+int64_t oracle_certify(const oracle_graph *g, const uint32_t *tris, uint64_t T, const int32_t *k,
+					   const uint32_t *rounds);
 
 #ifdef __cplusplus
 }

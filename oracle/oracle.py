@@ -61,6 +61,10 @@ def lib():
         L.oracle_count_triangles.restype = C.c_uint64
         L.oracle_count_k4.argtypes = [C.POINTER(OGraph)]
         L.oracle_count_k4.restype = C.c_uint64
+        L.oracle_peel_rounds.argtypes = [C.POINTER(OGraph), u32p, C.c_uint64, C.POINTER(C.c_int32), u32p]
+        L.oracle_peel_rounds.restype = C.c_int
+        L.oracle_certify.argtypes = [C.POINTER(OGraph), u32p, C.c_uint64, C.POINTER(C.c_int32), u32p]
+        L.oracle_certify.restype = C.c_int64
         _LIB = L
     return _LIB
 
@@ -162,3 +166,49 @@ def count_k4(g) -> int:
         return int(L.oracle_count_k4(C.byref(og)))
     finally:
         L.oracle_graph_free(C.byref(og))
+
+
+def _oriented(g):
+    D = np.ascontiguousarray(g.D, np.uint32)
+    E = np.ascontiguousarray(g.E if g.m else np.zeros(1, np.uint32), np.uint32)
+    og = OGraph()
+    rc = lib().oracle_graph_from_oriented(int(g.n), int(g.m), D.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                          E.ctypes.data_as(C.POINTER(C.c_uint32)), C.byref(og))
+    if rc:
+        raise RuntimeError(f"oracle_graph_from_oriented = {rc}")
+    return og
+
+
+def peel_rounds(g, tris: np.ndarray):
+    """Level-synchronous peel (the device peel's rules) on the canonical
+    triangle list: (k, death round) per triangle."""
+    T = len(tris)
+    t3 = np.ascontiguousarray(tris, np.uint32).reshape(-1)
+    k = np.zeros(max(T, 1), np.int32)
+    r = np.zeros(max(T, 1), np.uint32)
+    og = _oriented(g)
+    try:
+        rc = lib().oracle_peel_rounds(C.byref(og), t3.ctypes.data_as(C.POINTER(C.c_uint32)), T,
+                                      k.ctypes.data_as(C.POINTER(C.c_int32)), r.ctypes.data_as(C.POINTER(C.c_uint32)))
+        if rc:
+            raise RuntimeError(f"oracle_peel_rounds = {rc}")
+    finally:
+        lib().oracle_graph_free(C.byref(og))
+    return k[:T], r[:T]
+
+
+def certify(g, tris: np.ndarray, k: np.ndarray, rounds: np.ndarray) -> int:
+    """Number of triangles (and rounds) failing the certificate conditions."""
+    T = len(tris)
+    t3 = np.ascontiguousarray(tris, np.uint32).reshape(-1)
+    kk = np.ascontiguousarray(k, np.int32)
+    rr = np.ascontiguousarray(rounds, np.uint32)
+    og = _oriented(g)
+    try:
+        v = lib().oracle_certify(C.byref(og), t3.ctypes.data_as(C.POINTER(C.c_uint32)), T,
+                                 kk.ctypes.data_as(C.POINTER(C.c_int32)), rr.ctypes.data_as(C.POINTER(C.c_uint32)))
+    finally:
+        lib().oracle_graph_free(C.byref(og))
+    if v < 0:
+        raise RuntimeError(f"oracle_certify = {v}")
+    return int(v)
