@@ -248,14 +248,24 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 											   " exceeds the 32-bit position range");
 			break;
 		}
+		c.lean_run = false;
 		if (c.T)
 		{
-			// the on-demand peel with death flags (T < 2^30) keeps each
-			// triangle's entry positions
-			const bool want_tpos =
-				variant == NUCLEUS34_ONDEMAND && c.T <= 0x3fffffffull &&
-				!(c.opt_flags & (NUCLEUS34_OPT_STAMP_PEEL | NUCLEUS34_OPT_LEAN_MEMORY));
-			if ((rc = build_incidence(c, inc, want_tpos)))
+			// The on-demand peel with death flags (T < 2^30) uses either the
+			// regular layout (64-bit sort keys beside the entries, each
+			// triangle's entry positions, two frontier lists, k apart from the
+			// support: about 60 bytes per triangle at the incidence build) or,
+			// by request or when that does not fit in the memory left, the
+			// memory-lean one (entries sorted in place, no entry positions,
+			// bitmap frontiers, k kept in the support array: about 28 bytes
+			// per triangle beside the triangle list).
+			const bool flags_path = variant == NUCLEUS34_ONDEMAND && c.T <= 0x3fffffffull &&
+									!(c.opt_flags & NUCLEUS34_OPT_STAMP_PEEL);
+			const uint64_t room = c.budget > c.in_use ? c.budget - c.in_use : 0;
+			const uint64_t regular = 60 * c.T + 40 * c.m;
+			c.lean_run = flags_path && ((c.opt_flags & NUCLEUS34_OPT_LEAN_MEMORY) || regular > room);
+			const bool want_tpos = flags_path && !c.lean_run;
+			if ((rc = build_incidence(c, inc, want_tpos, c.lean_run)))
 				break;
 			r.sum_te_sq = inc.sum_te_sq;
 		}
@@ -294,7 +304,23 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 		if (variant == NUCLEUS34_DIRECT)
 			free_incidence(c, inc);
 		N34_CUDA(cudaEventRecord(ev.e[4], c.stream));
-		if (c.T)
+		if (c.T && c.lean_run)
+		{
+			// k is kept in the support array and becomes the result
+			if (total)
+			{
+				if ((rc = peel(c, variant, inc, csr, S, S, &pc)))
+					break;
+				peeled = true;
+			}
+			else
+			{
+				N34_LAUNCH(c, k_zero_k, grid_for(c, c.T, 256), 256, 0, S, c.T);
+			}
+			c.dK = S;
+			S = nullptr;
+		}
+		else if (c.T)
 		{
 			if ((rc = dalloc(c, &c.dK, c.T, "k values")))
 				break;

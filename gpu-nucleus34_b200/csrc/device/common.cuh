@@ -99,6 +99,7 @@ struct Ctx
 	std::string tune_table;
 	uint32_t opt_flags = 0;
 	double peel_debit_sec = 0; // profiling only: debit kernels' device time
+	bool lean_run = false;     // this run uses the memory-lean layout
 	std::mutex mu;
 
 	// resident graph

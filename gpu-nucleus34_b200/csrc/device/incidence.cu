@@ -24,6 +24,29 @@ namespace {
 constexpr int SEG_SMEM = 8192;        // keys per block sort (64 KB smem)
 constexpr int SEG_BLOCK = 512;
 
+// Entry storage of the sorts: the 64-bit (x<<32 | t) keys, or, in the
+// memory-lean build, the third[] and tri[] arrays themselves (sorted as pairs
+// in place, so that no key array coexists with them).
+struct EntryStore
+{
+	unsigned long long *keys; // null: use third / tri
+	uint32_t *third, *tri;
+	__device__ __forceinline__ unsigned long long ld(uint64_t i) const
+	{
+		return keys ? keys[i] : ((unsigned long long)third[i] << 32) | tri[i];
+	}
+	__device__ __forceinline__ void st(uint64_t i, unsigned long long v) const
+	{
+		if (keys)
+			keys[i] = v;
+		else
+		{
+			third[i] = uint32_t(v >> 32);
+			tri[i] = uint32_t(v);
+		}
+	}
+};
+
 __global__ void k_inc_count(const uint32_t *__restrict__ tris, uint64_t T, uint32_t *__restrict__ cnt)
 {
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
@@ -37,8 +60,8 @@ __global__ void k_inc_count(const uint32_t *__restrict__ tris, uint64_t T, uint3
 
 __global__ void k_inc_scatter(const uint32_t *__restrict__ tris, uint64_t T, const uint32_t *__restrict__ src,
 							  const uint32_t *__restrict__ E, const uint64_t *__restrict__ incO,
-							  uint32_t *__restrict__ cursor, unsigned long long *__restrict__ keys,
-							  uint32_t *__restrict__ err, bool slot_bits)
+							  uint32_t *__restrict__ cursor, EntryStore keys, uint32_t *__restrict__ err,
+							  bool slot_bits)
 {
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
@@ -54,7 +77,7 @@ __global__ void k_inc_scatter(const uint32_t *__restrict__ tris, uint64_t T, con
 			const uint32_t s = atomicAdd(cursor + e, 1u);
 			// capacity guard: the counts pass sized every segment exactly
 			if (incO[e] + s < incO[e + 1])
-				keys[incO[e] + s] = (uint64_t(x3[r]) << 32) | (slot_bits ? (t | (uint64_t(r) << 30)) : t);
+				keys.st(incO[e] + s, (uint64_t(x3[r]) << 32) | (slot_bits ? (t | (uint64_t(r) << 30)) : t));
 			else
 				atomicOr(err, 1u);
 		}
@@ -87,7 +110,7 @@ __global__ void k_seg_classify(const uint64_t *__restrict__ incO, uint64_t m, ui
 
 // Warp per segment (<= 32 entries): register bitonic network.
 __global__ void k_seg_sort_warp(const uint32_t *__restrict__ list, const uint32_t *__restrict__ count,
-								const uint64_t *__restrict__ incO, unsigned long long *__restrict__ keys)
+								const uint64_t *__restrict__ incO, EntryStore keys)
 {
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
@@ -97,7 +120,7 @@ __global__ void k_seg_sort_warp(const uint32_t *__restrict__ list, const uint32_
 	{
 		const uint32_t e = list[i];
 		const uint64_t b = incO[e], len = incO[e + 1] - b;
-		unsigned long long k = lane < len ? keys[b + lane] : ~0ull;
+		unsigned long long k = lane < len ? keys.ld(b + lane) : ~0ull;
 #pragma unroll
 		for (int size = 2; size <= 32; size <<= 1)
 		{
@@ -112,7 +135,7 @@ __global__ void k_seg_sort_warp(const uint32_t *__restrict__ list, const uint32_
 			}
 		}
 		if (lane < len)
-			keys[b + lane] = k;
+			keys.st(b + lane, k);
 	}
 }
 
@@ -141,7 +164,7 @@ __device__ __forceinline__ void block_bitonic(unsigned long long *s, uint32_t P)
 __global__ void __launch_bounds__(SEG_BLOCK) k_seg_sort_block(const uint32_t *__restrict__ list,
 															  const uint32_t *__restrict__ count,
 															  const uint64_t *__restrict__ incO,
-															  unsigned long long *__restrict__ keys)
+															  EntryStore keys)
 {
 	extern __shared__ unsigned long long sm[];
 	const uint32_t n = *count;
@@ -154,11 +177,11 @@ __global__ void __launch_bounds__(SEG_BLOCK) k_seg_sort_block(const uint32_t *__
 		while (P < len)
 			P <<= 1;
 		for (uint32_t j = threadIdx.x; j < P; j += blockDim.x)
-			sm[j] = j < len ? keys[b + j] : ~0ull;
+			sm[j] = j < len ? keys.ld(b + j) : ~0ull;
 		__syncthreads();
 		block_bitonic(sm, P);
 		for (uint32_t j = threadIdx.x; j < len; j += blockDim.x)
-			keys[b + j] = sm[j];
+			keys.st(b + j, sm[j]);
 		__syncthreads();
 	}
 }
@@ -167,7 +190,7 @@ __global__ void __launch_bounds__(SEG_BLOCK) k_seg_sort_block(const uint32_t *__
 __global__ void __launch_bounds__(SEG_BLOCK) k_seg_sort_global(const uint32_t *__restrict__ list,
 															   const uint32_t *__restrict__ count,
 															   const uint64_t *__restrict__ incO,
-															   unsigned long long *__restrict__ keys,
+															   EntryStore keys,
 															   unsigned long long *__restrict__ scratch,
 															   uint64_t region)
 {
@@ -184,11 +207,11 @@ __global__ void __launch_bounds__(SEG_BLOCK) k_seg_sort_global(const uint32_t *_
 		if (P > region)
 			continue; // cannot happen: region is sized from the longest segment
 		for (uint64_t j = threadIdx.x; j < P; j += blockDim.x)
-			s[j] = j < len ? keys[b + j] : ~0ull;
+			s[j] = j < len ? keys.ld(b + j) : ~0ull;
 		__syncthreads();
 		block_bitonic(s, uint32_t(P));
 		for (uint64_t j = threadIdx.x; j < len; j += blockDim.x)
-			keys[b + j] = s[j];
+			keys.st(b + j, s[j]);
 		__syncthreads();
 	}
 }
@@ -241,7 +264,7 @@ __global__ void k_make_spans(const uint64_t *__restrict__ off, uint64_t m, uint2
 
 } // namespace
 
-int build_incidence(Ctx &c, Incidence &inc, bool want_tpos)
+int build_incidence(Ctx &c, Incidence &inc, bool want_tpos, bool lean)
 {
 	const uint64_t T = c.T, m = c.m, n3 = 3 * T;
 	uint32_t *cnt = nullptr, *lists = nullptr, *counts = nullptr, *errf = nullptr;
@@ -274,8 +297,18 @@ int build_incidence(Ctx &c, Incidence &inc, bool want_tpos)
 		c.launches++;
 		if ((rc = scan_u32(c, cnt, off, m)))
 			break;
-		if ((rc = dalloc(c, &keys, n3, "incidence keys")))
+		// lean: the entries are scattered straight into third[] / tri[] and
+		// sorted there as pairs (no 8-byte key per entry beside them)
+		if (lean)
+		{
+			if ((rc = dalloc(c, &inc.third, n3, "incidence third")))
+				break;
+			if ((rc = dalloc(c, &inc.tri, n3, "incidence tri")))
+				break;
+		}
+		else if ((rc = dalloc(c, &keys, n3, "incidence keys")))
 			break;
+		const EntryStore store{keys, inc.third, inc.tri};
 		if (cudaMemsetAsync(cnt, 0, m * 4, c.stream) != cudaSuccess)
 		{
 			rc = fail(NUCLEUS34_E_CUDA, "memset");
@@ -290,7 +323,7 @@ int build_incidence(Ctx &c, Incidence &inc, bool want_tpos)
 		}
 		// entry positions per triangle (the on-demand peel's death flags);
 		// optional: without room for them the peel searches instead
-		if (want_tpos && T <= 0x3fffffffull)
+		if (want_tpos && !lean && T <= 0x3fffffffull)
 		{
 			if (dalloc(c, &inc.tpos, 3 * T, "triangle entry positions"))
 			{
@@ -298,7 +331,7 @@ int build_incidence(Ctx &c, Incidence &inc, bool want_tpos)
 				clear_error();
 			}
 		}
-		k_inc_scatter<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, c.dsrc, c.dE, off, cnt, keys, errf,
+		k_inc_scatter<<<grid_for(c, T, 256), 256, 0, c.stream>>>(c.dtris, T, c.dsrc, c.dE, off, cnt, store, errf,
 																 inc.tpos != nullptr);
 		c.launches++;
 		c.release(cnt);
@@ -342,7 +375,7 @@ int build_incidence(Ctx &c, Incidence &inc, bool want_tpos)
 		}
 		if (hcounts[0])
 		{
-			k_seg_sort_warp<<<grid_for(c, hcounts[0], 8, 32), 256, 0, c.stream>>>(lists, counts + 0, off, keys);
+			k_seg_sort_warp<<<grid_for(c, hcounts[0], 8, 32), 256, 0, c.stream>>>(lists, counts + 0, off, store);
 			c.launches++;
 		}
 		if (hcounts[1])
@@ -350,7 +383,7 @@ int build_incidence(Ctx &c, Incidence &inc, bool want_tpos)
 			const size_t smem = SEG_SMEM * sizeof(unsigned long long);
 			cudaFuncSetAttribute(k_seg_sort_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
 			k_seg_sort_block<<<grid_for(c, hcounts[1], 1, 2), SEG_BLOCK, smem, c.stream>>>(lists + m, counts + 1,
-																							off, keys);
+																							off, store);
 			c.launches++;
 		}
 		if (hcounts[2])
@@ -361,16 +394,19 @@ int build_incidence(Ctx &c, Incidence &inc, bool want_tpos)
 			const uint32_t blocks = std::min<uint32_t>(hcounts[2], uint32_t(c.sm_count));
 			if ((rc = dalloc(c, &scratch, P * blocks, "segment sort scratch")))
 				break;
-			k_seg_sort_global<<<blocks, SEG_BLOCK, 0, c.stream>>>(lists + 2 * m, counts + 2, off, keys,
+			k_seg_sort_global<<<blocks, SEG_BLOCK, 0, c.stream>>>(lists + 2 * m, counts + 2, off, store,
 																  scratch, P);
 			c.launches++;
 		}
-		if ((rc = dalloc(c, &inc.third, n3, "incidence third")))
-			break;
-		if ((rc = dalloc(c, &inc.tri, n3, "incidence tri")))
-			break;
-		k_inc_split<<<grid_for(c, n3, 256), 256, 0, c.stream>>>(keys, n3, inc.third, inc.tri, inc.tpos);
-		c.launches++;
+		if (!lean)
+		{
+			if ((rc = dalloc(c, &inc.third, n3, "incidence third")))
+				break;
+			if ((rc = dalloc(c, &inc.tri, n3, "incidence tri")))
+				break;
+			k_inc_split<<<grid_for(c, n3, 256), 256, 0, c.stream>>>(keys, n3, inc.third, inc.tri, inc.tpos);
+			c.launches++;
+		}
 		if ((rc = dalloc(c, &inc.span, m ? m : 1, "incidence spans")))
 			break;
 		k_make_spans<<<grid_for(c, m, 256), 256, 0, c.stream>>>(off, m, inc.span);

@@ -56,11 +56,77 @@ struct CtlX
 	unsigned long long st_tri, st_merge_entries, st_steps, st_lookups, st_resolves, st_staged, st_found;
 };
 
+// A frontier is a list F[0, nF) (default) or, in the memory-lean peel, a
+// bitmap of T bits (one u32 word per 32 triangles; no list at all). Two of
+// each alternate between the current and the next round.
+struct Frontier
+{
+	uint32_t *F0, *F1; // lists (null in bitmap mode)
+	uint32_t *B0, *B1; // bitmaps (null in list mode)
+	uint64_t W;        // bitmap words
+	__device__ __forceinline__ bool bits() const { return B0 != nullptr; }
+	__device__ __forceinline__ uint32_t *cur_list(uint32_t cur) const { return cur ? F1 : F0; }
+	__device__ __forceinline__ uint32_t *next_list(uint32_t cur) const { return cur ? F0 : F1; }
+	__device__ __forceinline__ uint32_t *cur_bits(uint32_t cur) const { return cur ? B1 : B0; }
+	__device__ __forceinline__ uint32_t *next_bits(uint32_t cur) const { return cur ? B0 : B1; }
+};
+
+// f(t) for every triangle of the current frontier, grid-stride over threads;
+// in bitmap mode one thread takes one word, and with clear it zeroes the
+// word afterwards (the last kernel of a round frees the bitmap for reuse).
+template <class Fn>
+__device__ __forceinline__ void frontier_each_thread(const Frontier fr, uint32_t cur, uint32_t nF, bool clear,
+													 Fn &&f)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	const uint64_t tid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+	if (fr.bits())
+	{
+		uint32_t *B = fr.cur_bits(cur);
+		for (uint64_t w = tid; w < fr.W; w += stride)
+		{
+			uint32_t word = B[w];
+			if (!word)
+				continue;
+			if (clear)
+				B[w] = 0;
+			while (word)
+			{
+				const uint32_t b = __ffs(word) - 1;
+				word &= word - 1;
+				f(uint32_t(w * 32 + b));
+			}
+		}
+	}
+	else
+	{
+		const uint32_t *F = fr.cur_list(cur);
+		for (uint64_t i = tid; i < nF; i += stride)
+			f(F[i]);
+	}
+}
+
+// Adds triangle q to the next frontier (list append or bit), counting nNext.
+__device__ __forceinline__ void frontier_push(const Frontier fr, uint32_t cur, uint32_t q, uint32_t *nNext,
+											  uint64_t cap, uint32_t *err)
+{
+	const uint32_t slot = atomicAdd(nNext, 1u);
+	if (fr.bits())
+		atomicOr(fr.next_bits(cur) + (q >> 5), 1u << (q & 31));
+	else if (slot < cap)
+		fr.next_list(cur)[slot] = q;
+	else
+		atomicOr(err, 1u);
+}
+
+// K null: k is kept in S (a dead triangle holds -1 - k there), as in the
+// memory-lean peel; otherwise every k starts at -1 (not peeled).
 __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
 {
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
-		K[t] = -1;
+	if (K)
+		for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
+			K[t] = -1;
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 	{
 		PeelCtl z{};
@@ -81,26 +147,38 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
 // Level change (frontier empty): every alive triangle has S > level, and dead
 // ones hold S = INT_MAX. First try the next level directly (the usual case);
 // only if nothing sits at level+1 compute the minimum and gather at it.
+// Dead triangles hold S = -1 - k < 0; live supports are never negative.
+__device__ __forceinline__ void gather_take(const Frontier fr, CtlX *ctl, bool take, uint64_t t, uint64_t T)
+{
+	const uint32_t slot = warp_append(take, &ctl->c.nF);
+	if (take)
+	{
+		if (fr.bits())
+			atomicOr(fr.cur_bits(ctl->c.cur) + (t >> 5), 1u << (t & 31));
+		else if (slot < T)
+			fr.cur_list(ctl->c.cur)[slot] = uint32_t(t);
+		else
+			atomicOr(&ctl->c.error, 1u);
+	}
+}
+
 __global__ void __launch_bounds__(PEEL_THREADS) k_gather_next(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T,
-															  uint32_t *__restrict__ F0, uint32_t *__restrict__ F1)
+															  Frontier fr)
 {
 	if (ctl->c.done || !ctl->scan)
 		return;
 	const int32_t want = int32_t(ctl->c.level) + 1;
-	uint32_t *F = ctl->c.cur ? F1 : F0;
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < T; t0 += stride)
 	{
 		const uint64_t t = t0 + threadIdx.x;
-		const bool take = t < T && S[t] <= want;
-		const uint32_t slot = warp_append(take, &ctl->c.nF);
-		if (take)
+		bool take = false;
+		if (t < T)
 		{
-			if (slot < T)
-				F[slot] = uint32_t(t);
-			else
-				atomicOr(&ctl->c.error, 1u);
+			const int32_t s = S[t];
+			take = s >= 0 && s <= want;
 		}
+		gather_take(fr, ctl, take, t, T);
 	}
 }
 
@@ -120,8 +198,8 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int3
 	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
 	{
 		const int32_t s = S[t];
-		if (s != INT32_MAX)
-			mn = min(mn, uint32_t(s < 0 ? 0 : s));
+		if (s >= 0)
+			mn = min(mn, uint32_t(s));
 	}
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1)
@@ -132,7 +210,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int3
 
 // Second chance of the level change: gather at the minimum (or finish).
 __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T,
-														 uint32_t *__restrict__ F0, uint32_t *__restrict__ F1)
+														 Frontier fr)
 {
 	if (ctl->c.done || !ctl->scan)
 		return;
@@ -152,7 +230,6 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_
 	// every alive triangle sits above the old level, so the minimum is the new one
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		ctl->c.level = mn;
-	uint32_t *F = ctl->c.cur ? F1 : F0;
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < T; t0 += stride)
 	{
@@ -161,16 +238,9 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_
 		if (t < T)
 		{
 			const int32_t s = S[t];
-			take = s != INT32_MAX && uint32_t(s < 0 ? 0 : s) <= mn;
+			take = s >= 0 && uint32_t(s) <= mn;
 		}
-		const uint32_t slot = warp_append(take, &ctl->c.nF);
-		if (take)
-		{
-			if (slot < T)
-				F[slot] = uint32_t(t);
-			else
-				atomicOr(&ctl->c.error, 1u);
-		}
+		gather_take(fr, ctl, take, t, T);
 	}
 }
 
@@ -189,7 +259,7 @@ __global__ void k_mark(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_
 		const uint32_t t = F[i];
 		K[t] = level;
 		R[t] = round;
-		S[t] = INT32_MAX; // dead: out of every later scan (dead triangles are never debited)
+		S[t] = -1 - level; // dead: out of every later scan (dead triangles are never debited)
 	}
 }
 
@@ -428,25 +498,20 @@ __device__ __forceinline__ void entry_positions(uint32_t t, const uint32_t *__re
 	pos[2] = lower_bound32(third, sc.x, sc.y, u);
 }
 
-__global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
-							 int32_t *__restrict__ K, int32_t *__restrict__ S, const uint32_t *__restrict__ tris,
-							 const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
-							 const uint2 *__restrict__ span, const uint32_t *__restrict__ third,
-							 const uint32_t *__restrict__ tpos, uint32_t *__restrict__ itri, uint64_t n3,
-							 uint32_t *__restrict__ R)
+__global__ void k_mark_flags(CtlX *ctl, Frontier fr, int32_t *__restrict__ K, int32_t *__restrict__ S,
+							 const uint32_t *__restrict__ tris, const uint32_t *__restrict__ src,
+							 const uint32_t *__restrict__ E, const uint2 *__restrict__ span,
+							 const uint32_t *__restrict__ third, const uint32_t *__restrict__ tpos,
+							 uint32_t *__restrict__ itri, uint64_t n3, uint32_t *__restrict__ R)
 {
 	if (ctl->c.done)
 		return;
-	const uint32_t nF = ctl->c.nF;
-	const uint32_t *F = ctl->c.cur ? F1 : F0;
 	const int32_t level = int32_t(ctl->c.level);
 	const uint32_t round = ctl->c.round;
-	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nF; i += stride)
-	{
-		const uint32_t t = F[i];
-		K[t] = level;
-		S[t] = INT32_MAX;
+	frontier_each_thread(fr, ctl->c.cur, ctl->c.nF, false, [&](uint32_t t) {
+		if (K)
+			K[t] = level;
+		S[t] = -1 - level; // dead from now on: out of every later scan
 		if (R)
 			R[t] = round;
 		uint64_t pos[3];
@@ -455,30 +520,25 @@ __global__ void k_mark_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const u
 		for (int r = 0; r < 3; ++r)
 			if (pos[r] < n3)
 				itri[pos[r]] = t | DYING;
-	}
+	});
 }
 
-__global__ void k_finalize_flags(CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
-								 const uint32_t *__restrict__ tris, const uint32_t *__restrict__ src,
-								 const uint32_t *__restrict__ E, const uint2 *__restrict__ span,
-								 const uint32_t *__restrict__ third, const uint32_t *__restrict__ tpos,
-								 uint32_t *__restrict__ itri, uint64_t n3)
+__global__ void k_finalize_flags(CtlX *ctl, Frontier fr, const uint32_t *__restrict__ tris,
+								 const uint32_t *__restrict__ src, const uint32_t *__restrict__ E,
+								 const uint2 *__restrict__ span, const uint32_t *__restrict__ third,
+								 const uint32_t *__restrict__ tpos, uint32_t *__restrict__ itri, uint64_t n3)
 {
 	if (ctl->c.done)
 		return;
-	const uint32_t nF = ctl->c.nF;
-	const uint32_t *F = ctl->c.cur ? F1 : F0;
-	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < nF; i += stride)
-	{
-		const uint32_t t = F[i];
+	// the round's last frontier kernel: a bitmap frontier is cleared here
+	frontier_each_thread(fr, ctl->c.cur, ctl->c.nF, true, [&](uint32_t t) {
 		uint64_t pos[3];
 		entry_positions(t, tris, src, E, span, third, tpos, pos);
 #pragma unroll
 		for (int r = 0; r < 3; ++r)
 			if (pos[r] < n3)
 				itri[pos[r]] = t | DEAD;
-	}
+	});
 }
 
 // Owner rule on flagged entries: q0..q2 are the three partners' entries (no
@@ -505,25 +565,19 @@ __device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q
 // of a partner that died earlier is gone; a third that is not found on an edge
 // therefore means the clique was destroyed before.
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
-	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
-	const uint2 *__restrict__ span, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
-	int32_t *__restrict__ S, uint64_t T)
+	CtlX *ctl, Frontier fr, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
+	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T)
 {
 	if (ctl->c.done)
 		return;
-	const uint32_t nF = ctl->c.nF;
-	const uint32_t *F = ctl->c.cur ? F1 : F0;
-	uint32_t *Fn = ctl->c.cur ? F0 : F1;
+	const uint32_t cur = ctl->c.cur;
 	const int32_t level = int32_t(ctl->c.level);
 	uint32_t *nNext = &ctl->c.nNext;
 	uint32_t *err = &ctl->c.error;
-	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-	for (uint64_t fi = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; fi < nF; fi += stride)
-	{
-		const uint32_t t = F[fi];
+	frontier_each_thread(fr, cur, ctl->c.nF, false, [&](uint32_t t) {
 		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 > THREAD_MODE_MAX)
-			continue; // the warp kernel takes it
+			return; // the warp kernel takes it
 		uint32_t lo_b = L.b0, lo_c = L.c0;
 		for (uint32_t i = L.a0; i < L.a1 && lo_b < L.b1; ++i)
 		{
@@ -551,15 +605,9 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 #pragma unroll
 			for (int r = 0; r < 3; ++r)
 				if (hit[r])
-				{
-					const uint32_t slot = atomicAdd(nNext, 1u);
-					if (slot < T)
-						Fn[slot] = qs[r];
-					else
-						atomicOr(err, 1u);
-				}
+					frontier_push(fr, cur, qs[r], nNext, T, err);
 		}
-	}
+	});
 }
 
 // Debit of dying triangles with long lists: one warp each, tile merge (or
@@ -582,10 +630,11 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 #ifndef N34_DEBIT_MINB
 #define N34_DEBIT_MINB 6
 #endif
+template <bool BITS>
 __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_warp(
-	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, const uint32_t *__restrict__ tris,
-	const uint2 *__restrict__ span, const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
-	int32_t *__restrict__ S, uint64_t T)
+	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
+	uint32_t *__restrict__ B1, uint64_t W, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
+	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T)
 {
 	constexpr int WARPS = PEEL_THREADS / 32;
 	__shared__ uint32_t qx[WARPS][64], qp0[WARPS][64], qp1[WARPS][64];
@@ -594,9 +643,8 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 #endif
 	if (ctl->c.done)
 		return;
-	const uint32_t nF = ctl->c.nF;
-	const uint32_t *F = ctl->c.cur ? F1 : F0;
 	uint32_t *Fn = ctl->c.cur ? F0 : F1;
+	uint32_t *Bn = ctl->c.cur ? B0 : B1;
 	const int32_t level = int32_t(ctl->c.level);
 	uint32_t *nNext = &ctl->c.nNext;
 	uint32_t *err = &ctl->c.error;
@@ -604,9 +652,35 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 	uint32_t *bx = qx[wib], *b0 = qp0[wib], *b1 = qp1[wib];
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
-	for (uint64_t fi = warp; fi < nF; fi += nwarps)
+	const uint32_t nF = ctl->c.nF;
+	const uint32_t *F = ctl->c.cur ? F1 : F0;
+	const uint32_t *Bc = ctl->c.cur ? B1 : B0;
+	uint32_t word = 0; // bits of word fi not yet taken (bitmap mode)
+	// fi: list position, or bitmap word, advanced by the bitmap branch itself
+	for (uint64_t fi = warp;; fi += (BITS ? 0 : nwarps))
 	{
-		const uint32_t t = F[fi];
+		uint32_t t;
+		if (BITS)
+		{
+			while (!word && fi < W)
+			{
+				word = Bc[fi];
+				if (!word)
+					fi += nwarps;
+			}
+			if (!word)
+				break;
+			t = uint32_t(fi * 32 + (__ffs(word) - 1));
+			word &= word - 1;
+			if (!word)
+				fi += nwarps;
+		}
+		else
+		{
+			if (fi >= nF)
+				break;
+			t = F[fi];
+		}
 		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 <= THREAD_MODE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
@@ -714,7 +788,9 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 				const uint32_t slot = warp_append(hit[r], nNext);
 				if (hit[r])
 				{
-					if (slot < T)
+					if (BITS)
+						atomicOr(Bn + (qs[r] >> 5), 1u << (qs[r] & 31));
+					else if (slot < T)
 						Fn[slot] = qs[r];
 					else
 						atomicOr(err, 1u);
@@ -1041,6 +1117,13 @@ __global__ void k_advance(CtlX *ctl)
 	ctl->scan = c.nF == 0;
 }
 
+__global__ void k_s_to_k(int32_t *__restrict__ S, uint64_t T)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
+		S[t] = -1 - S[t];
+}
+
 __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 {
 	unsigned long long sum = 0;
@@ -1080,7 +1163,8 @@ __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_t *S, int32_t *K, PeelCtl *hctl)
 {
 	const uint64_t T = c.T;
-	uint32_t *R = nullptr, *F0 = nullptr, *F1 = nullptr, *fbits = nullptr, *fchunk = nullptr;
+	uint32_t *R = nullptr, *F0 = nullptr, *F1 = nullptr, *B0 = nullptr, *B1 = nullptr, *fbits = nullptr,
+			 *fchunk = nullptr;
 	uint8_t *destroyed = nullptr;
 	CtlX *ctl = nullptr;
 	int rc = NUCLEUS34_OK;
@@ -1088,6 +1172,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		c.release(R);
 		c.release(F0);
 		c.release(F1);
+		c.release(B0);
+		c.release(B1);
 		c.release(fbits);
 		c.release(fchunk);
 		c.release(ctl);
@@ -1099,20 +1185,47 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 	// death rounds: the round-stamp owner test needs them; the death-flag
 	// path records them only to keep them for nucleus34_ctx_verify
 	const bool keep_rounds = (c.opt_flags & NUCLEUS34_OPT_VERIFIABLE) != 0;
+	// Memory-lean peel (death-flag path only): frontiers as two bitmaps of T
+	// bits instead of two lists of T ids, and, when the caller passes K == S,
+	// k kept in S (a dead triangle holds -1 - k) and converted at the end.
+	const bool lean = flags && c.lean_run;
+	const bool k_in_s = (K == S);
+	int32_t *Kw = k_in_s ? nullptr : K;
+	const uint64_t fwords = (T + 31) / 32;
 	do
 	{
+		if (k_in_s && !lean)
+		{
+			rc = fail(NUCLEUS34_E_INVALID, "internal: k kept in S outside the lean peel");
+			break;
+		}
 		if ((!flags || keep_rounds) && (rc = dalloc(c, &R, T, "peel round stamps")))
 			break;
-		if ((rc = dalloc(c, &F0, T, "frontier 0")))
-			break;
-		if ((rc = dalloc(c, &F1, T, "frontier 1")))
-			break;
+		if (lean)
+		{
+			if ((rc = dalloc(c, &B0, fwords, "frontier bitmap 0")) || (rc = dalloc(c, &B1, fwords, "frontier bitmap 1")))
+				break;
+			if (cudaMemsetAsync(B0, 0, fwords * 4, c.stream) != cudaSuccess ||
+				cudaMemsetAsync(B1, 0, fwords * 4, c.stream) != cudaSuccess)
+			{
+				rc = fail(NUCLEUS34_E_CUDA, "memset");
+				break;
+			}
+		}
+		else
+		{
+			if ((rc = dalloc(c, &F0, T, "frontier 0")))
+				break;
+			if ((rc = dalloc(c, &F1, T, "frontier 1")))
+				break;
+		}
+		const Frontier fr{F0, F1, B0, B1, fwords};
 		if ((rc = dalloc(c, &ctl, 1, "peel control")))
 			break;
-		// frontier ordering bitmap (optional: skipped without room for it)
-		const uint64_t fwords = (T + 31) / 32;
+		// frontier ordering bitmap (optional: skipped without room for it;
+		// a bitmap frontier is in id order already)
 		const uint64_t fchunks = (fwords + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
-		if ((c.opt_flags & NUCLEUS34_OPT_LEAN_MEMORY) || dalloc(c, &fbits, fwords, "frontier order bitmap") ||
+		if (lean || (c.opt_flags & NUCLEUS34_OPT_LEAN_MEMORY) || dalloc(c, &fbits, fwords, "frontier order bitmap") ||
 			dalloc(c, &fchunk, fchunks, "frontier order chunks"))
 		{
 			c.release(fbits);
@@ -1139,7 +1252,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		}
 		const uint32_t gscan = grid_for(c, T, PEEL_THREADS, 8);
 		const uint32_t gwarp = grid_for(c, T, PEEL_THREADS / 32, 16);
-		k_peel_init<<<gscan, PEEL_THREADS, 0, c.stream>>>(K, T, ctl);
+		k_peel_init<<<gscan, PEEL_THREADS, 0, c.stream>>>(Kw, T, ctl);
 		c.launches++;
 		{
 			const uint32_t on = (c.opt_flags & NUCLEUS34_OPT_PROFILE_PEEL) ? 1u : 0u;
@@ -1162,26 +1275,30 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 					cudaEventRecord(ev[j], c.stream);
 			};
 			tick(0);
-			k_gather_next<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, F0, F1);
+			k_gather_next<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, fr);
 			tick(1);
 			k_scan_min<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T);
 			tick(2);
-			k_gather<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, F0, F1);
+			k_gather<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, fr);
 			tick(3);
 			if (trace)
 				cudaMemcpyAsync(trace, &ctl->c, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream);
 			if (flags)
 			{
-				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, K, S, c.dtris, c.dsrc, c.dE, inc.span,
+				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, Kw, S, c.dtris, c.dsrc, c.dE, inc.span,
 																   inc.third, inc.tpos, inc.tri, 3 * T, R);
 				tick(4);
-				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.span,
-																		   inc.third, inc.tri, S, T);
+				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, inc.span, inc.third,
+																		   inc.tri, S, T);
 				tick(5);
-				k_debit_flags_warp<<<gwarp, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, inc.span, inc.third,
-																		 inc.tri, S, T);
+				if (lean)
+					k_debit_flags_warp<true><<<gwarp, PEEL_THREADS, 0, c.stream>>>(
+						ctl, F0, F1, B0, B1, fwords, c.dtris, inc.span, inc.third, inc.tri, S, T);
+				else
+					k_debit_flags_warp<false><<<gwarp, PEEL_THREADS, 0, c.stream>>>(
+						ctl, F0, F1, B0, B1, fwords, c.dtris, inc.span, inc.third, inc.tri, S, T);
 				tick(6);
-				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, c.dtris, c.dsrc, c.dE, inc.span,
+				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, c.dsrc, c.dE, inc.span,
 																	   inc.third, inc.tpos, inc.tri, 3 * T);
 				tick(7);
 			}
@@ -1377,6 +1494,12 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			cudaGraphDestroy(graph);
 		if (rc)
 			break;
+		if (k_in_s)
+		{
+			// -1 - k of every peeled triangle back to k (unpeeled ones stay negative)
+			k_s_to_k<<<gscan, PEEL_THREADS, 0, c.stream>>>(S, T);
+			c.launches++;
+		}
 		k_stats<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, K, T);
 		c.launches++;
 		if (cudaMemcpyAsync(hctl, &ctl->c, sizeof(PeelCtl), cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||

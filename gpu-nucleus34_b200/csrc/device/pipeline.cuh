@@ -38,7 +38,8 @@ cudaError_t launch_tri_count(const uint32_t *O, const uint32_t *E, uint64_t n, u
 cudaError_t launch_tri_write(const uint32_t *O, const uint32_t *E, uint64_t n, const uint64_t *toff,
 							 uint32_t *tris, int sm_count, cudaStream_t s);
 int list_triangles(Ctx &c);
-int build_incidence(Ctx &c, Incidence &inc, bool want_tpos);
+// lean: no 64-bit key array (entries sorted in place as pairs) and no tpos.
+int build_incidence(Ctx &c, Incidence &inc, bool want_tpos, bool lean = false);
 void free_incidence(Ctx &c, Incidence &inc);
 // support[t] = number of four-cliques on t; returns sum(support) in *total.
 // own (optional): cliques whose lowest triangle is t (direct variant sizes).

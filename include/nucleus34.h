@@ -81,10 +81,13 @@ typedef struct
  * every step and print per-step device times to stderr (diagnostics only;
  * slower than the default graph replay). */
 #define NUCLEUS34_OPT_PROFILE_PEEL 0x2u
-/* opts.flags: allocate none of the optional speed-up arrays (per-triangle
- * entry positions, frontier-order bitmap); the peel then searches for a
- * triangle's entries and keeps frontiers in append order. The same arrays
- * are skipped automatically when the memory budget has no room for them. */
+/* opts.flags: the memory-lean layout of the on-demand variant (T < 2^30):
+ * incidence entries sorted in place (no 64-bit sort keys beside them), no
+ * per-triangle entry positions (the peel searches for a triangle's entries),
+ * frontiers as two bitmaps instead of two lists, and k kept in the support
+ * array; about 28 bytes per triangle beside the triangle list instead of
+ * about 60. Chosen automatically when the regular layout does not fit in
+ * the memory budget left after the triangle listing. Results are identical. */
 #define NUCLEUS34_OPT_LEAN_MEMORY 0x4u
 /* opts.flags: keep each triangle's death round after the peel, so that
  * nucleus34_ctx_verify can certify the result (costs 4 bytes per triangle). */

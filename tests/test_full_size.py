@@ -65,3 +65,25 @@ def test_rgg4m_certified_and_cliques_counted_independently(n34, oracle):
     assert r["k_max"] == 35
     assert viol == 0 and checked == r["triangle_count"]
     assert r["four_clique_count"] == oracle.count_k4(g)
+
+
+def test_rgg4m_under_a_40gb_budget_matches_the_uncapped_run(n34):
+    """The on-demand config with device memory capped at 40 GB: the library
+    switches to its memory-lean layout (entries sorted in place, bitmap
+    frontiers, k kept in the support array) and must give the uncapped run's
+    results bit for bit, within the cap."""
+    s, t = n34.gen_rgg(4000000, 48.0, 3)
+    g = n34.graph_from_edges(s, t)
+    with n34.Context() as ctx:
+        ctx.upload(g)
+        free = ctx.run("ondemand")
+        k_free = ctx.copy_k(int(free["triangle_count"]))
+    budget = 40 * 10**9
+    with n34.Context(mem_budget_bytes=budget) as ctx:
+        ctx.upload(g)
+        lean = ctx.run("ondemand")
+        k_lean = ctx.copy_k(int(lean["triangle_count"]))
+    assert lean["peak_device_bytes"] <= budget < free["peak_device_bytes"]
+    for key in ("triangle_count", "four_clique_count", "k_max", "k_avg"):
+        assert lean[key] == free[key], key
+    assert np.array_equal(k_lean, k_free)

@@ -116,8 +116,9 @@ def test_stamp_peel_path_matches(n34, oracle, case):
 
 @pytest.mark.parametrize("case", [("rmat", 13, 16, 3), ("rgg", 30000, 40, 9)])
 def test_lean_and_profiled_peels_match(n34, oracle, case):
-    """Without the optional arrays (entries searched, frontiers unordered) and
-    with the per-step profiling launches, k is the same."""
+    """In the memory-lean layout (entries sorted in place, entries searched,
+    bitmap frontiers, k kept in the support array) and with the per-step
+    profiling launches, k is the same."""
     if case[0] == "rmat":
         s, t = n34.gen_rmat(case[1], case[2], case[3])
     else:
