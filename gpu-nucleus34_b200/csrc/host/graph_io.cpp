@@ -104,46 +104,96 @@ int build_oriented(const uint32_t *src, const uint32_t *dst, uint64_t count, Hos
 			max_node = std::max(max_node, std::max(src[i], dst[i]));
 	const uint64_t n = uint64_t(max_node) + 1;
 
-	// undirected CSR by counting sort on the source, both directions
-	std::vector<uint64_t> off(n + 1, 0);
+	// Undirected CSR, both directions, built in buckets of 2^SH vertices so
+	// that every write stays in cache: each thread counts and then scatters
+	// its slice of the pairs into the buckets' regions (the entry carries its
+	// source's low SH bits), and each bucket is then counting-sorted by source
+	// in place, where its lists are sorted and deduplicated.
+	constexpr uint32_t SH = 12;
+	const uint64_t nb = (n >> SH) + 1;
+	const int nth = std::max(1, omp_get_max_threads());
+	std::vector<uint64_t> cursor(uint64_t(nth) * nb, 0);
+#pragma omp parallel num_threads(nth)
 	{
-		std::vector<std::atomic<uint32_t>> deg(n);
-#pragma omp parallel for schedule(static)
-		for (int64_t v = 0; v < int64_t(n); ++v)
-			deg[v].store(0, std::memory_order_relaxed);
-#pragma omp parallel for schedule(static)
-		for (int64_t i = 0; i < int64_t(count); ++i)
+		const int t = omp_get_thread_num();
+		const uint64_t lo = count * uint64_t(t) / uint64_t(nth), hi = count * uint64_t(t + 1) / uint64_t(nth);
+		uint64_t *h = cursor.data() + uint64_t(t) * nb;
+		for (uint64_t i = lo; i < hi; ++i)
 			if (src[i] != dst[i])
 			{
-				deg[src[i]].fetch_add(1, std::memory_order_relaxed);
-				deg[dst[i]].fetch_add(1, std::memory_order_relaxed);
+				h[src[i] >> SH]++;
+				h[dst[i] >> SH]++;
 			}
-		for (uint64_t v = 0; v < n; ++v)
-			off[v + 1] = off[v] + deg[v].load(std::memory_order_relaxed);
 	}
-	const uint64_t total = off[n];
+	std::vector<uint64_t> bstart(nb + 1, 0);
+	uint64_t run = 0;
+	for (uint64_t b = 0; b < nb; ++b)
+	{
+		bstart[b] = run;
+		for (int t = 0; t < nth; ++t)
+		{
+			const uint64_t c = cursor[uint64_t(t) * nb + b];
+			cursor[uint64_t(t) * nb + b] = run;
+			run += c;
+		}
+	}
+	bstart[nb] = run;
+	const uint64_t total = run;
 	std::vector<uint32_t> adj(total ? total : 1);
+	std::vector<uint16_t> low(total ? total : 1);
+#pragma omp parallel num_threads(nth)
 	{
-		std::vector<std::atomic<uint64_t>> cur(n);
-#pragma omp parallel for schedule(static)
-		for (int64_t v = 0; v < int64_t(n); ++v)
-			cur[v].store(off[v], std::memory_order_relaxed);
-#pragma omp parallel for schedule(static)
-		for (int64_t i = 0; i < int64_t(count); ++i)
-			if (src[i] != dst[i])
-			{
-				adj[cur[src[i]].fetch_add(1, std::memory_order_relaxed)] = dst[i];
-				adj[cur[dst[i]].fetch_add(1, std::memory_order_relaxed)] = src[i];
-			}
+		const int t = omp_get_thread_num();
+		const uint64_t lo = count * uint64_t(t) / uint64_t(nth), hi = count * uint64_t(t + 1) / uint64_t(nth);
+		uint64_t *h = cursor.data() + uint64_t(t) * nb;
+		constexpr uint32_t MASK = (1u << SH) - 1;
+		for (uint64_t i = lo; i < hi; ++i)
+		{
+			const uint32_t u = src[i], v = dst[i];
+			if (u == v)
+				continue;
+			uint64_t p = h[u >> SH]++;
+			adj[p] = v;
+			low[p] = uint16_t(u & MASK);
+			p = h[v >> SH]++;
+			adj[p] = u;
+			low[p] = uint16_t(v & MASK);
+		}
 	}
+	std::vector<uint64_t> off(n + 1, 0);
+	off[n] = total;
 	// per-list sort + unique == global pair sort + unique (graph.hpp:383-388)
 	std::vector<uint32_t> udeg(n, 0);
-#pragma omp parallel for schedule(dynamic, 256)
-	for (int64_t v = 0; v < int64_t(n); ++v)
+#pragma omp parallel num_threads(nth)
 	{
-		uint32_t *b = adj.data() + off[v], *e = adj.data() + off[v + 1];
-		std::sort(b, e);
-		udeg[v] = uint32_t(std::unique(b, e) - b);
+		std::vector<uint64_t> cnt((1u << SH) + 1);
+		std::vector<uint32_t> tmp;
+#pragma omp for schedule(dynamic, 4)
+		for (int64_t b = 0; b < int64_t(nb); ++b)
+		{
+			const uint64_t s0 = bstart[b], e0 = bstart[b + 1];
+			const uint64_t v0 = uint64_t(b) << SH;
+			const uint64_t nv = std::min<uint64_t>(uint64_t(1) << SH, n - std::min(n, v0));
+			std::fill(cnt.begin(), cnt.end(), 0);
+			for (uint64_t p = s0; p < e0; ++p)
+				cnt[low[p] + 1]++;
+			for (uint64_t j = 0; j < nv; ++j)
+			{
+				cnt[j + 1] += cnt[j];
+				off[v0 + j] = s0 + cnt[j];
+			}
+			tmp.resize(e0 - s0);
+			for (uint64_t p = s0; p < e0; ++p)
+				tmp[cnt[low[p]]++] = adj[p];
+			std::copy(tmp.begin(), tmp.end(), adj.begin() + s0);
+			for (uint64_t j = 0; j < nv; ++j)
+			{
+				uint32_t *lb = adj.data() + off[v0 + j];
+				uint32_t *le = adj.data() + (j + 1 < nv ? off[v0 + j + 1] : e0);
+				std::sort(lb, le);
+				udeg[v0 + j] = uint32_t(std::unique(lb, le) - lb);
+			}
+		}
 	}
 	// orientation on the undirected degree (graph.hpp:196-213)
 	out.n = n;

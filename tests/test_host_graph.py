@@ -103,3 +103,17 @@ def test_rmat_scale12_matches_configured_size(n34):
     assert 45_000 <= len(s) <= 50_000
     h = hashlib.sha256(s.tobytes() + d.tobytes()).hexdigest()
     assert h  # pinned indirectly through tests/golden (input_sha256)
+
+
+def test_bucketed_csr_build_matches_the_oracle_on_large_inputs(n34, oracle):
+    """The CSR build works in buckets of 4096 vertices; graphs spanning many
+    buckets, with self-loops and duplicate pairs, give the oracle's CSR."""
+    rng = np.random.default_rng(3)
+    cases = [n34.gen_rgg(200000, 20.0, 5), n34.gen_rmat(16, 12, 9)]
+    s = rng.integers(0, 50000, 300000).astype(np.uint32)
+    d = np.where(rng.random(300000) < 0.1, s, rng.integers(0, 50000, 300000)).astype(np.uint32)
+    cases.append((np.concatenate([s, s[:1000]]), np.concatenate([d, d[:1000]])))
+    for s, d in cases:
+        a = n34.graph_from_edges(s, d)
+        b = oracle.graph_from_pairs(s, d)
+        assert a.n == b.n and np.array_equal(a.D, b.D) and np.array_equal(a.E, b.E)
