@@ -18,7 +18,11 @@
 #include <string>
 #include <vector>
 
+#include <fcntl.h>
 #include <omp.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 namespace n34 {
 
@@ -94,36 +98,94 @@ int read_file(const char *path, std::vector<char> &buf)
 
 } // namespace
 
-int build_oriented(const uint32_t *src, const uint32_t *dst, uint64_t count, HostGraph &out)
+namespace {
+
+// A text file mapped read-only (or, where mapping fails, read into memory).
+struct MappedText
 {
+	const char *data = nullptr;
+	size_t size = 0;
+	void *map = nullptr;
+	std::vector<char> copy;
+	int open(const char *path)
+	{
+		const int fd = ::open(path, O_RDONLY);
+		if (fd < 0)
+			return fail(NUCLEUS34_E_IO, std::string("Dataset ") + path + " is not accessible!");
+		struct stat st;
+		if (fstat(fd, &st) == 0 && st.st_size > 0)
+		{
+			void *m = mmap(nullptr, size_t(st.st_size), PROT_READ, MAP_PRIVATE, fd, 0);
+			if (m != MAP_FAILED)
+			{
+				madvise(m, size_t(st.st_size), MADV_SEQUENTIAL);
+				map = m;
+				data = static_cast<const char *>(m);
+				size = size_t(st.st_size);
+				::close(fd);
+				return NUCLEUS34_OK;
+			}
+		}
+		::close(fd);
+		const int rc = read_file(path, copy);
+		data = copy.data();
+		size = copy.size();
+		return rc;
+	}
+	~MappedText()
+	{
+		if (map)
+			munmap(map, size);
+	}
+};
+
+// A slice of the input pairs; the parser hands over its per-thread slices
+// as they are, without concatenating them.
+struct PairSlice
+{
+	const uint32_t *src, *dst;
+	uint64_t count;
+};
+
+int build_oriented_slices(const std::vector<PairSlice> &parts, HostGraph &out)
+{
+	const int nth = std::max(1, omp_get_max_threads());
+	const int64_t np = int64_t(parts.size());
 	// max_node over non-self-loop pairs only (graph.hpp:365-369)
 	uint32_t max_node = 0;
-#pragma omp parallel for reduction(max : max_node) schedule(static)
-	for (int64_t i = 0; i < int64_t(count); ++i)
-		if (src[i] != dst[i])
-			max_node = std::max(max_node, std::max(src[i], dst[i]));
+#pragma omp parallel for reduction(max : max_node) schedule(dynamic, 1) num_threads(nth)
+	for (int64_t pi = 0; pi < np; ++pi)
+	{
+		const PairSlice &ps = parts[size_t(pi)];
+		for (uint64_t i = 0; i < ps.count; ++i)
+			if (ps.src[i] != ps.dst[i])
+				max_node = std::max(max_node, std::max(ps.src[i], ps.dst[i]));
+	}
 	const uint64_t n = uint64_t(max_node) + 1;
 
 	// Undirected CSR, both directions, built in buckets of 2^SH vertices so
 	// that every write stays in cache: each thread counts and then scatters
-	// its slice of the pairs into the buckets' regions (the entry carries its
+	// its slices of the pairs into the buckets' regions (the entry carries its
 	// source's low SH bits), and each bucket is then counting-sorted by source
-	// in place, where its lists are sorted and deduplicated.
+	// in place, where its lists are sorted and deduplicated. Thread t takes
+	// slices t, t + nth, ... in both passes.
 	constexpr uint32_t SH = 12;
 	const uint64_t nb = (n >> SH) + 1;
-	const int nth = std::max(1, omp_get_max_threads());
 	std::vector<uint64_t> cursor(uint64_t(nth) * nb, 0);
 #pragma omp parallel num_threads(nth)
 	{
 		const int t = omp_get_thread_num();
-		const uint64_t lo = count * uint64_t(t) / uint64_t(nth), hi = count * uint64_t(t + 1) / uint64_t(nth);
 		uint64_t *h = cursor.data() + uint64_t(t) * nb;
-		for (uint64_t i = lo; i < hi; ++i)
-			if (src[i] != dst[i])
-			{
-				h[src[i] >> SH]++;
-				h[dst[i] >> SH]++;
-			}
+		for (int64_t pi = t; pi < np; pi += nth)
+		{
+			const PairSlice &ps = parts[size_t(pi)];
+			for (uint64_t i = 0; i < ps.count; ++i)
+				if (ps.src[i] != ps.dst[i])
+				{
+					h[ps.src[i] >> SH]++;
+					h[ps.dst[i] >> SH]++;
+				}
+		}
 	}
 	std::vector<uint64_t> bstart(nb + 1, 0);
 	uint64_t run = 0;
@@ -144,20 +206,23 @@ int build_oriented(const uint32_t *src, const uint32_t *dst, uint64_t count, Hos
 #pragma omp parallel num_threads(nth)
 	{
 		const int t = omp_get_thread_num();
-		const uint64_t lo = count * uint64_t(t) / uint64_t(nth), hi = count * uint64_t(t + 1) / uint64_t(nth);
 		uint64_t *h = cursor.data() + uint64_t(t) * nb;
 		constexpr uint32_t MASK = (1u << SH) - 1;
-		for (uint64_t i = lo; i < hi; ++i)
+		for (int64_t pi = t; pi < np; pi += nth)
 		{
-			const uint32_t u = src[i], v = dst[i];
-			if (u == v)
-				continue;
-			uint64_t p = h[u >> SH]++;
-			adj[p] = v;
-			low[p] = uint16_t(u & MASK);
-			p = h[v >> SH]++;
-			adj[p] = u;
-			low[p] = uint16_t(v & MASK);
+			const PairSlice &ps = parts[size_t(pi)];
+			for (uint64_t i = 0; i < ps.count; ++i)
+			{
+				const uint32_t u = ps.src[i], v = ps.dst[i];
+				if (u == v)
+					continue;
+				uint64_t p = h[u >> SH]++;
+				adj[p] = v;
+				low[p] = uint16_t(u & MASK);
+				p = h[v >> SH]++;
+				adj[p] = u;
+				low[p] = uint16_t(v & MASK);
+			}
 		}
 	}
 	std::vector<uint64_t> off(n + 1, 0);
@@ -236,6 +301,20 @@ int build_oriented(const uint32_t *src, const uint32_t *dst, uint64_t count, Hos
 	return NUCLEUS34_OK;
 }
 
+} // namespace
+
+int build_oriented(const uint32_t *src, const uint32_t *dst, uint64_t count, HostGraph &out)
+{
+	const uint64_t nth = uint64_t(std::max(1, omp_get_max_threads()));
+	std::vector<PairSlice> parts;
+	for (uint64_t t = 0; t < nth; ++t)
+	{
+		const uint64_t lo = count * t / nth, hi = count * (t + 1) / nth;
+		parts.push_back(PairSlice{src + lo, dst + lo, hi - lo});
+	}
+	return build_oriented_slices(parts, out);
+}
+
 int load_graph(const char *path, HostGraph &g)
 {
 	if (!path)
@@ -279,11 +358,12 @@ int load_graph(const char *path, HostGraph &g)
 	if (!mtx && ext != ".edges" && ext != ".txt")
 		return fail(NUCLEUS34_E_FORMAT, "Unknown dataset format: " + ext);
 
-	std::vector<char> buf;
-	int rc = read_file(path, buf);
+	// the text is mapped, not copied (a read into memory is the fallback)
+	MappedText text;
+	int rc = text.open(path);
 	if (rc)
 		return rc;
-	const char *p = buf.data(), *end = buf.data() + buf.size();
+	const char *p = text.data, *end = text.data + text.size;
 
 	// Skip leading comment lines: a line whose first character is '#' or '%'
 	// (graph.hpp:307-314). The first other line is the header: parsed for
@@ -354,6 +434,9 @@ int load_graph(const char *path, HostGraph &g)
 		const char *q = cb[c], *qe = cb[c + 1];
 		auto &S = ps[c];
 		auto &Dd = pd[c];
+		// a pair line has at least 4 characters ("1 2\n"): no reallocation
+		S.reserve(size_t(qe - q) / 4 + 1);
+		Dd.reserve(size_t(qe - q) / 4 + 1);
 		while (q < qe)
 		{
 			const char *nl = static_cast<const char *>(std::memchr(q, '\n', size_t(qe - q)));
@@ -367,17 +450,11 @@ int load_graph(const char *path, HostGraph &g)
 			q = nl ? nl + 1 : qe;
 		}
 	}
-	std::vector<uint64_t> coff(nchunks + 1, 0);
+	// the parsed chunks go to the CSR build in file order, as they are
+	std::vector<PairSlice> parts(static_cast<size_t>(nchunks));
 	for (int c = 0; c < nchunks; ++c)
-		coff[c + 1] = coff[c] + ps[c].size();
-	std::vector<uint32_t> S(coff[nchunks]), Dd(coff[nchunks]);
-#pragma omp parallel for schedule(dynamic, 1)
-	for (int c = 0; c < nchunks; ++c)
-	{
-		std::copy(ps[c].begin(), ps[c].end(), S.begin() + coff[c]);
-		std::copy(pd[c].begin(), pd[c].end(), Dd.begin() + coff[c]);
-	}
-	return build_oriented(S.data(), Dd.data(), S.size(), g);
+		parts[size_t(c)] = PairSlice{ps[c].data(), pd[c].data(), ps[c].size()};
+	return build_oriented_slices(parts, g);
 }
 
 int save_grh(const nucleus34_graph *g, const char *path)
