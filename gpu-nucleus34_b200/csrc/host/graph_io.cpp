@@ -19,6 +19,7 @@
 #include <vector>
 
 #include <fcntl.h>
+#include <memory>
 #include <omp.h>
 #include <sys/mman.h>
 #include <sys/stat.h>
@@ -32,33 +33,50 @@ bool is_digit(char c) { return c >= '0' && c <= '9'; }
 
 // "<uint> <uint>" at the start of a line, as `ss >> s >> d` reads well-formed
 // input (graph.hpp:361-363). Lines without two numbers are skipped (the
-// reference reads uninitialised values for them).
-inline bool parse_two(const char *p, const char *end, uint32_t &s, uint32_t &d)
+// reference reads uninitialised values for them). Reads from p up to end and
+// reports where it stopped; the caller skips the rest of the line from there.
+// A line's numbers cannot run past its newline: '\n' is neither a digit, a
+// space nor a tab.
+inline bool parse_two_at(const char *p, const char *end, uint32_t &s, uint32_t &d, const char *&stop)
 {
+	stop = p;
 	while (p < end && (*p == ' ' || *p == '\t'))
 		++p;
 	if (p >= end || !is_digit(*p))
+	{
+		stop = p;
 		return false;
+	}
 	uint64_t a = 0;
 	while (p < end && is_digit(*p))
 	{
 		a = a * 10 + uint64_t(*p - '0');
 		if (a > 0xffffffffull)
+		{
+			stop = p;
 			return false;
+		}
 		++p;
 	}
 	while (p < end && (*p == ' ' || *p == '\t'))
 		++p;
 	if (p >= end || !is_digit(*p))
+	{
+		stop = p;
 		return false;
+	}
 	uint64_t b = 0;
 	while (p < end && is_digit(*p))
 	{
 		b = b * 10 + uint64_t(*p - '0');
 		if (b > 0xffffffffull)
+		{
+			stop = p;
 			return false;
+		}
 		++p;
 	}
+	stop = p;
 	s = uint32_t(a);
 	d = uint32_t(b);
 	return true;
@@ -427,33 +445,42 @@ int load_graph(const char *path, HostGraph &g)
 		const char *nl = static_cast<const char *>(std::memchr(q, '\n', size_t(end - q)));
 		cb[c] = nl ? nl + 1 : end;
 	}
-	std::vector<std::vector<uint32_t>> ps(nchunks), pd(nchunks);
+	// Each chunk parses into its own uninitialised buffers, sized for the
+	// most pair lines it can hold (a pair line has at least 4 characters,
+	// "1 2\n"). The two numbers are read in one pass from the line start
+	// (parse_two stops at the first character that is neither a digit, a
+	// space nor a tab, so the bound is the chunk end), then the rest of the
+	// line is skipped.
+	std::vector<std::unique_ptr<uint32_t[]>> ps(nchunks), pd(nchunks);
+	std::vector<uint64_t> pn(nchunks, 0);
 #pragma omp parallel for schedule(dynamic, 1)
 	for (int c = 0; c < nchunks; ++c)
 	{
 		const char *q = cb[c], *qe = cb[c + 1];
-		auto &S = ps[c];
-		auto &Dd = pd[c];
-		// a pair line has at least 4 characters ("1 2\n"): no reallocation
-		S.reserve(size_t(qe - q) / 4 + 1);
-		Dd.reserve(size_t(qe - q) / 4 + 1);
+		const size_t cap = size_t(qe - q) / 4 + 1;
+		ps[c].reset(new uint32_t[cap]);
+		pd[c].reset(new uint32_t[cap]);
+		uint32_t *S = ps[c].get(), *Dd = pd[c].get();
+		uint64_t k = 0;
 		while (q < qe)
 		{
-			const char *nl = static_cast<const char *>(std::memchr(q, '\n', size_t(qe - q)));
-			const char *le = nl ? nl : qe;
+			const char *stop = q;
 			uint32_t s, d;
-			if (parse_two(q, le, s, d))
+			if (parse_two_at(q, qe, s, d, stop))
 			{
-				S.push_back(s);
-				Dd.push_back(d);
+				S[k] = s;
+				Dd[k] = d;
+				++k;
 			}
+			const char *nl = static_cast<const char *>(std::memchr(stop, '\n', size_t(qe - stop)));
 			q = nl ? nl + 1 : qe;
 		}
+		pn[c] = k;
 	}
 	// the parsed chunks go to the CSR build in file order, as they are
 	std::vector<PairSlice> parts(static_cast<size_t>(nchunks));
 	for (int c = 0; c < nchunks; ++c)
-		parts[size_t(c)] = PairSlice{ps[c].data(), pd[c].data(), ps[c].size()};
+		parts[size_t(c)] = PairSlice{ps[c].get(), pd[c].get(), pn[c]};
 	return build_oriented_slices(parts, g);
 }
 
