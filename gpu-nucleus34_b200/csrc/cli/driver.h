@@ -77,6 +77,10 @@ inline int run_program(const ProgramSpec &spec, int argc, char **argv)
 		nucleus34_opts opts{};
 		opts.device = 0;
 		opts.parts = uint32_t(parts);
+		// scheduling table of the on-demand variant (argv stays the reference's)
+		const char *tune = std::getenv("NUCLEUS34_TUNE_TABLE");
+		if (tune && *tune)
+			opts.tune_table = tune;
 		nucleus34_result r{};
 		const nucleus34_csr csr = nucleus34_graph_csr(&g);
 		int rc = spec.direct ? nucleus34_decompose(&csr, &opts, &r, &h) : nucleus34_decompose_ondemand(&csr, &opts, &r, &h);

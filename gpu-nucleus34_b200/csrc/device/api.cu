@@ -154,6 +154,7 @@ void Ctx::release_graph()
 	release(dsrc);
 	dO = dE = dsrc = nullptr;
 	n = m = 0;
+	max_out = 0;
 }
 
 int upload(Ctx &c, const nucleus34_csr *csr)
@@ -169,12 +170,14 @@ int upload(Ctx &c, const nucleus34_csr *csr)
 	const uint64_t n = csr->n, m = csr->m;
 	std::vector<uint32_t> O(n + 1);
 	uint64_t s = 0;
+	uint32_t max_out = 0;
 	for (uint64_t u = 0; u < n; ++u)
 	{
 		if (csr->O && csr->O[u] != s)
 			return fail(NUCLEUS34_E_INVALID, "O is not the exclusive scan of D");
 		O[u] = uint32_t(s);
 		s += csr->D[u];
+		max_out = csr->D[u] > max_out ? csr->D[u] : max_out;
 	}
 	if (s != m)
 		return fail(NUCLEUS34_E_INVALID, "sum of D does not equal m");
@@ -187,6 +190,7 @@ int upload(Ctx &c, const nucleus34_csr *csr)
 		N34_CUDA(cudaMemcpyAsync(c.dE, csr->E, m * 4, cudaMemcpyHostToDevice, c.stream));
 	c.n = n;
 	c.m = m;
+	c.max_out = max_out;
 	uint32_t *bad = nullptr;
 	N34_TRY(dalloc(c, &bad, 1, "validation flag"));
 	N34_CUDA(cudaMemsetAsync(bad, 0, 4, c.stream));
@@ -205,6 +209,28 @@ int upload(Ctx &c, const nucleus34_csr *csr)
 	N34_TRY(build_src(c));
 	N34_CUDA(cudaStreamSynchronize(c.stream));
 	return NUCLEUS34_OK;
+}
+
+// Settings of this run: the direct variant keeps the defaults (its clique
+// order must not depend on them); the on-demand one takes the pinned
+// settings, else the tune table's line for the graph's class, else the
+// defaults. Called once T is known.
+void select_tune(Ctx &c, int variant)
+{
+	c.tune = tune_filled(nucleus34_tune{});
+	if (variant != NUCLEUS34_ONDEMAND)
+		return;
+	if (c.tune_pinned)
+	{
+		c.tune = tune_filled(c.tune_pin);
+		return;
+	}
+	if (c.tune_rules.empty())
+		return;
+	int32_t size = 0, skew = 0;
+	tune_class(c.T, c.n, c.m, c.max_out, size, skew);
+	if (const TuneRule *r = tune_match(c.tune_rules, size, skew))
+		c.tune = tune_filled(r->tune);
 }
 
 int run(Ctx &c, int variant, nucleus34_result *out)
@@ -240,6 +266,7 @@ int run(Ctx &c, int variant, nucleus34_result *out)
 		N34_CUDA(cudaEventRecord(ev.e[1], c.stream));
 		r.triangle_count = c.T;
 		r.incidence_entries = 3 * c.T;
+		select_tune(c, variant);
 		// The incidence is addressed with 32-bit positions, the limit the
 		// reference also enforces (cuNucleus34_ondemand.cu:505-511).
 		if (3 * c.T > 0xffffffffull)
@@ -387,6 +414,111 @@ int copy_k(Ctx &c, int32_t *k_out, uint32_t *tris_out)
 	return NUCLEUS34_OK;
 }
 
+// Autotuner: coordinate descent over the settings of the on-demand variant.
+// Every trial is a full run whose k is compared with the default run's.
+int autotune(Ctx &c, const char *path, nucleus34_tune *best_out, double *best_sec, double *default_sec)
+{
+	if (!c.dO)
+		return fail(NUCLEUS34_E_STATE, "no graph uploaded");
+	const bool pinned0 = c.tune_pinned;
+	const nucleus34_tune pin0 = c.tune_pin;
+	std::vector<int32_t> ref, got;
+	nucleus34_result r0{};
+	bool have_ref = false;
+	// one run under t, timed on the device (t_total); the first one sets the
+	// reference result
+	auto trial = [&](const nucleus34_tune &t, double &sec) -> int {
+		c.tune_pinned = true;
+		c.tune_pin = t;
+		nucleus34_result r{};
+		N34_TRY(run(c, NUCLEUS34_ONDEMAND, &r));
+		sec = r.t_total;
+		std::vector<int32_t> &dst = have_ref ? got : ref;
+		dst.resize(c.T);
+		N34_TRY(copy_k(c, dst.data(), nullptr));
+		if (!have_ref)
+		{
+			r0 = r;
+			have_ref = true;
+		}
+		else if (r.triangle_count != r0.triangle_count || r.four_clique_count != r0.four_clique_count ||
+				 got != ref)
+			return fail(NUCLEUS34_E_CUDA, "autotune: the settings " + tune_line(TuneRule{0, 0, t, 0, 0, 0}) +
+											  " changed the result");
+		return NUCLEUS34_OK;
+	};
+	auto body = [&]() -> int {
+		const nucleus34_tune def = tune_filled(nucleus34_tune{});
+		double s0 = 0, s1 = 0, s2 = 0;
+		N34_TRY(trial(def, s0)); // warm-up and reference
+		N34_TRY(trial(def, s1));
+		N34_TRY(trial(def, s2));
+		const double t_def = std::min(s1, s2);
+		nucleus34_tune best = def;
+		double t_best = t_def;
+		const uint32_t NEVER = NUCLEUS34_TUNE_NEVER;
+		const std::vector<uint32_t> lanes = {8, 16, 32}, divs = {4, 8, 16, NEVER}, shifts = {10, 12, 14, NEVER},
+									rounds = {8, 16, 32};
+		using Member = uint32_t nucleus34_tune::*;
+		struct Field
+		{
+			Member f;
+			const std::vector<uint32_t> *values;
+		};
+		const Field fields[] = {{&nucleus34_tune::lane_max, &lanes},
+								{&nucleus34_tune::compact_div, &divs},
+								{&nucleus34_tune::sort_shift, &shifts},
+								{&nucleus34_tune::rounds_per_replay, &rounds}};
+		for (const Field &fd : fields)
+			for (uint32_t v : *fd.values)
+			{
+				if (best.*fd.f == v)
+					continue;
+				nucleus34_tune cand = best;
+				cand.*fd.f = v;
+				double a = 0, b = 0;
+				N34_TRY(trial(cand, a));
+				if (a >= 0.99 * t_best)
+					continue;
+				N34_TRY(trial(cand, b)); // confirm: both runs 1% faster
+				if (b >= 0.99 * t_best)
+					continue;
+				best = cand;
+				t_best = 0.5 * (a + b);
+			}
+		if (best_out)
+			*best_out = best;
+		if (best_sec)
+			*best_sec = t_best;
+		if (default_sec)
+			*default_sec = t_def;
+		if (path)
+		{
+			TuneRule rule;
+			tune_class(c.T, c.n, c.m, c.max_out, rule.size, rule.skew);
+			rule.tune = best;
+			rule.sec = t_best;
+			rule.default_sec = t_def;
+			N34_TRY(tune_store(path, rule));
+			// later unpinned runs of this context use the new line too
+			bool replaced = false;
+			for (auto &x : c.tune_rules)
+				if (x.size == rule.size && x.skew == rule.skew)
+				{
+					x = rule;
+					replaced = true;
+				}
+			if (!replaced)
+				c.tune_rules.push_back(rule);
+		}
+		return NUCLEUS34_OK;
+	};
+	const int rc = body();
+	c.tune_pinned = pinned0;
+	c.tune_pin = pin0;
+	return rc;
+}
+
 int write_kfile(Ctx &c, const char *path)
 {
 	std::vector<int32_t> k(c.T);
@@ -436,6 +568,10 @@ int create_ctx(const nucleus34_opts *opts, nucleus34_ctx *out)
 	}
 	if (dev < 0 || dev >= ndev)
 		return fail(NUCLEUS34_E_INVALID, "device ordinal out of range");
+	// a tune table is read and checked up front: a bad one fails the call
+	std::vector<TuneRule> rules;
+	if (opts && opts->tune_table)
+		N34_TRY(tune_read(opts->tune_table, rules));
 	cudaDeviceProp prop{};
 	N34_CUDA(cudaGetDeviceProperties(&prop, dev));
 	if (prop.major < 10)
@@ -446,6 +582,7 @@ int create_ctx(const nucleus34_opts *opts, nucleus34_ctx *out)
 		return fail(NUCLEUS34_E_INVALID, "host allocation failed");
 	Ctx &c = x->c;
 	c.device = dev;
+	c.tune_rules = std::move(rules);
 	c.sm_count = prop.multiProcessorCount;
 	if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess)
 	{
@@ -477,8 +614,6 @@ int create_ctx(const nucleus34_opts *opts, nucleus34_ctx *out)
 		cudaGetLastError();
 	}
 	c.budget = (opts && opts->mem_budget_bytes) ? opts->mem_budget_bytes : uint64_t(double(fb + cached) * 0.9);
-	if (opts && opts->tune_table)
-		c.tune_table = opts->tune_table;
 	if (opts)
 		c.opt_flags = opts->flags;
 	*out = x;
@@ -603,6 +738,42 @@ int nucleus34_ctx_copy_k(nucleus34_ctx ctx, int32_t *k_out, uint32_t *tris_out)
 }
 
 void nucleus34_ctx_destroy(nucleus34_ctx ctx) { destroy_ctx(ctx); }
+
+int nucleus34_ctx_set_tune(nucleus34_ctx ctx, const nucleus34_tune *tune)
+{
+	if (!ctx)
+		return fail(NUCLEUS34_E_INVALID, "null context");
+	return guarded([&]() -> int {
+		if (tune)
+			N34_TRY(tune_check(*tune));
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		ctx->c.tune_pinned = tune != nullptr;
+		ctx->c.tune_pin = tune ? *tune : nucleus34_tune{};
+		return NUCLEUS34_OK;
+	});
+}
+
+int nucleus34_ctx_last_tune(nucleus34_ctx ctx, nucleus34_tune *out)
+{
+	if (!ctx || !out)
+		return fail(NUCLEUS34_E_INVALID, "null argument");
+	return guarded([&]() -> int {
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		*out = tune_filled(ctx->c.tune);
+		return NUCLEUS34_OK;
+	});
+}
+
+int nucleus34_ctx_autotune(nucleus34_ctx ctx, const char *path, nucleus34_tune *best, double *best_sec,
+						   double *default_sec)
+{
+	if (!ctx)
+		return fail(NUCLEUS34_E_INVALID, "null context");
+	return guarded([&] {
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		return autotune(ctx->c, path, best, best_sec, default_sec);
+	});
+}
 
 int nucleus34_ctx_verify(nucleus34_ctx ctx, uint64_t *violations, uint64_t *checked)
 {

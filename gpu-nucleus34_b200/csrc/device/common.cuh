@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "nucleus34.h"
+#include "tune.h"
 
 namespace n34 {
 
@@ -96,7 +97,10 @@ struct Ctx
 	uint64_t in_use = 0;
 	uint64_t peak = 0;
 	uint64_t launches = 0;
-	std::string tune_table;
+	std::vector<TuneRule> tune_rules; // the context's tune table (empty: defaults)
+	bool tune_pinned = false;         // settings pinned by nucleus34_ctx_set_tune
+	nucleus34_tune tune_pin{};
+	nucleus34_tune tune = tune_filled(nucleus34_tune{}); // settings of the current / last run
 	uint32_t opt_flags = 0;
 	double peel_debit_sec = 0; // profiling only: debit kernels' device time
 	bool lean_run = false;     // this run uses the memory-lean layout
@@ -104,6 +108,7 @@ struct Ctx
 
 	// resident graph
 	uint64_t n = 0, m = 0;
+	uint32_t max_out = 0;   // maximum out-degree (the tune table's skew class)
 	uint32_t *dO = nullptr; // n+1
 	uint32_t *dE = nullptr; // m
 	uint32_t *dsrc = nullptr; // m

@@ -38,9 +38,6 @@ namespace {
 
 constexpr uint32_t INF = 0xffffffffu;
 constexpr int PEEL_THREADS = 256;
-#ifndef N34_COMPACT_DIV
-#define N34_COMPACT_DIV 8
-#endif
 
 struct CtlX
 {
@@ -48,6 +45,8 @@ struct CtlX
 	uint32_t scan;        // 1 while the next frontier must come from a scan
 	uint32_t next_found;  // k_scan_min's snapshot: k_gather_next found a frontier
 	uint32_t compact_now; // set by k_compact_gate for the replay's compaction
+	uint32_t compact_div; // compaction gate divisor (0: never compact)
+	unsigned long long sort_min; // frontiers at least this large are put in id order
 	unsigned long long peeled_at_compact;
 	unsigned long long live_at_compact;
 	uint32_t compactions;
@@ -121,7 +120,8 @@ __device__ __forceinline__ void frontier_push(const Frontier fr, uint32_t cur, u
 
 // K null: k is kept in S (a dead triangle holds -1 - k there), as in the
 // memory-lean peel; otherwise every k starts at -1 (not peeled).
-__global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
+__global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl, uint32_t compact_div,
+							unsigned long long sort_min)
 {
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	if (K)
@@ -136,6 +136,8 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl)
 		ctl->scan = 1;
 		ctl->next_found = 0;
 		ctl->compact_now = 0;
+		ctl->compact_div = compact_div;
+		ctl->sort_min = sort_min;
 		ctl->peeled_at_compact = 0;
 		ctl->live_at_compact = T;
 		ctl->compactions = 0;
@@ -564,6 +566,7 @@ __device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q
 // shortest list are skipped before any search. After a compaction the entry
 // of a partner that died earlier is gone; a third that is not found on an edge
 // therefore means the clique was destroyed before.
+template <uint32_t LANE_MAX>
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	CtlX *ctl, Frontier fr, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
 	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T)
@@ -576,7 +579,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	uint32_t *err = &ctl->c.error;
 	frontier_each_thread(fr, cur, ctl->c.nF, false, [&](uint32_t t) {
 		const Lists L = frontier_lists(t, tris, span);
-		if (L.a1 - L.a0 > THREAD_MODE_MAX)
+		if (L.a1 - L.a0 > LANE_MAX)
 			return; // the warp kernel takes it
 		uint32_t lo_b = L.b0, lo_c = L.c0;
 		for (uint32_t i = L.a0; i < L.a1 && lo_b < L.b1; ++i)
@@ -630,7 +633,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 #ifndef N34_DEBIT_MINB
 #define N34_DEBIT_MINB 6
 #endif
-template <bool BITS>
+template <bool BITS, uint32_t LANE_MAX>
 __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
 	uint32_t *__restrict__ B1, uint64_t W, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
@@ -682,7 +685,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 			t = F[fi];
 		}
 		const Lists L = frontier_lists(t, tris, span);
-		if (L.a1 - L.a0 <= THREAD_MODE_MAX)
+		if (L.a1 - L.a0 <= LANE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
 #if N34_L2_PREFETCH
 		if (lane == 0 && use_merge(L))
@@ -857,12 +860,10 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 // Ordering of large frontiers. Appends leave the next frontier in random
 // order; the debit of a random order reads every dying triangle's lists from
 // DRAM, while in id order (edge-major, as the triangles are numbered)
-// neighbouring warps share lists in L2. A frontier of at least T >> SORT_SHIFT
-// triangles is therefore rewritten in id order through a bitmap: set bits,
-// count per chunk, scan the counts, write the ids back (clearing the bits).
-#ifndef N34_SORT_SHIFT
-#define N34_SORT_SHIFT 12
-#endif
+// neighbouring warps share lists in L2. A frontier of at least
+// max(T >> sort_shift, SORT_MIN) triangles (ctl->sort_min) is therefore
+// rewritten in id order through a bitmap: set bits, count per chunk, scan the
+// counts, write the ids back (clearing the bits).
 #ifndef N34_SORT_MIN
 #define N34_SORT_MIN 4096ull
 #endif
@@ -871,8 +872,7 @@ constexpr int SORT_THREADS = 256;
 
 __device__ __forceinline__ bool sort_wanted(const CtlX *ctl, uint64_t T)
 {
-	const uint64_t thr = (T >> N34_SORT_SHIFT) > N34_SORT_MIN ? (T >> N34_SORT_SHIFT) : N34_SORT_MIN;
-	return !ctl->c.done && ctl->c.nNext >= thr && ctl->c.nNext <= T;
+	return !ctl->c.done && ctl->c.nNext >= ctl->sort_min && ctl->c.nNext <= T;
 }
 
 __global__ void k_fsort_set(const CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
@@ -1032,9 +1032,9 @@ __global__ void __launch_bounds__(SORT_THREADS) k_fsort_write(const CtlX *ctl, u
 }
 
 // Compaction gate, run after each replay: once the triangles peeled since
-// the last compaction reach 1/N34_COMPACT_DIV of the live ones then, the next
+// the last compaction reach 1/compact_div of the live ones then, the next
 // k_compact_spans drops the dead entries. A compaction reads every remaining
-// entry once, so the passes form a geometric series (at most N34_COMPACT_DIV
+// entry once, so the passes form a geometric series (at most compact_div
 // passes over the full incidence in total).
 __global__ void k_compact_gate(CtlX *ctl, uint64_t T)
 {
@@ -1042,7 +1042,8 @@ __global__ void k_compact_gate(CtlX *ctl, uint64_t T)
 	ctl->compact_now = 0;
 	if (ctl->c.done || peeled >= T)
 		return;
-	if (N34_COMPACT_DIV * (peeled - ctl->peeled_at_compact) >= ctl->live_at_compact)
+	if (ctl->compact_div &&
+		(unsigned long long)ctl->compact_div * (peeled - ctl->peeled_at_compact) >= ctl->live_at_compact)
 	{
 		ctl->compact_now = 1;
 		ctl->peeled_at_compact = peeled;
@@ -1158,6 +1159,23 @@ __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 	}
 }
 
+// The two debit kernels of the death-flag peel with one lane/warp split
+// (LM); ev5 (profiling only) is recorded between them.
+template <uint32_t LM>
+void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool lean, CtlX *ctl, const Frontier &fr,
+						const uint32_t *tris, const Incidence &inc, int32_t *S, uint64_t T, cudaEvent_t ev5)
+{
+	k_debit_flags_thread<LM><<<gscan, PEEL_THREADS, 0, st>>>(ctl, fr, tris, inc.span, inc.third, inc.tri, S, T);
+	if (ev5)
+		cudaEventRecord(ev5, st);
+	if (lean)
+		k_debit_flags_warp<true, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
+																	 inc.span, inc.third, inc.tri, S, T);
+	else
+		k_debit_flags_warp<false, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
+																	  inc.span, inc.third, inc.tri, S, T);
+}
+
 } // namespace
 
 int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_t *S, int32_t *K, PeelCtl *hctl)
@@ -1192,6 +1210,13 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 	const bool k_in_s = (K == S);
 	int32_t *Kw = k_in_s ? nullptr : K;
 	const uint64_t fwords = (T + 31) / 32;
+	// scheduling settings of this run (identical results for any of them)
+	const nucleus34_tune tn = tune_filled(c.tune);
+	const bool sort_on = tn.sort_shift != NUCLEUS34_TUNE_NEVER;
+	const unsigned long long sort_min =
+		sort_on ? std::max<unsigned long long>(T >> tn.sort_shift, N34_SORT_MIN) : ~0ull;
+	const uint32_t compact_div = tn.compact_div == NUCLEUS34_TUNE_NEVER ? 0u : tn.compact_div;
+	const uint32_t rpr = tn.rounds_per_replay;
 	do
 	{
 		if (k_in_s && !lean)
@@ -1225,7 +1250,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		// frontier ordering bitmap (optional: skipped without room for it;
 		// a bitmap frontier is in id order already)
 		const uint64_t fchunks = (fwords + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
-		if (lean || (c.opt_flags & NUCLEUS34_OPT_LEAN_MEMORY) || dalloc(c, &fbits, fwords, "frontier order bitmap") ||
+		if (!sort_on || lean || (c.opt_flags & NUCLEUS34_OPT_LEAN_MEMORY) ||
+			dalloc(c, &fbits, fwords, "frontier order bitmap") ||
 			dalloc(c, &fchunk, fchunks, "frontier order chunks"))
 		{
 			c.release(fbits);
@@ -1252,7 +1278,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		}
 		const uint32_t gscan = grid_for(c, T, PEEL_THREADS, 8);
 		const uint32_t gwarp = grid_for(c, T, PEEL_THREADS / 32, 16);
-		k_peel_init<<<gscan, PEEL_THREADS, 0, c.stream>>>(Kw, T, ctl);
+		k_peel_init<<<gscan, PEEL_THREADS, 0, c.stream>>>(Kw, T, ctl, compact_div, sort_min);
 		c.launches++;
 		{
 			const uint32_t on = (c.opt_flags & NUCLEUS34_OPT_PROFILE_PEEL) ? 1u : 0u;
@@ -1288,15 +1314,15 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				k_mark_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, Kw, S, c.dtris, c.dsrc, c.dE, inc.span,
 																   inc.third, inc.tpos, inc.tri, 3 * T, R);
 				tick(4);
-				k_debit_flags_thread<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, inc.span, inc.third,
-																		   inc.tri, S, T);
-				tick(5);
-				if (lean)
-					k_debit_flags_warp<true><<<gwarp, PEEL_THREADS, 0, c.stream>>>(
-						ctl, F0, F1, B0, B1, fwords, c.dtris, inc.span, inc.third, inc.tri, S, T);
+				cudaEvent_t ev5 = ev ? ev[5] : nullptr;
+				static_assert(THREAD_MODE_MAX == TUNE_LANE_MAX, "default lane/warp split");
+				if (tn.lane_max == 8)
+					launch_debit_flags<8>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5);
+				else if (tn.lane_max == 32)
+					launch_debit_flags<32>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5);
 				else
-					k_debit_flags_warp<false><<<gwarp, PEEL_THREADS, 0, c.stream>>>(
-						ctl, F0, F1, B0, B1, fwords, c.dtris, inc.span, inc.third, inc.tri, S, T);
+					launch_debit_flags<THREAD_MODE_MAX>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T,
+														ev5);
 				tick(6);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, c.dsrc, c.dE, inc.span,
 																	   inc.third, inc.tpos, inc.tri, 3 * T);
@@ -1329,26 +1355,26 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				cudaEventRecord(ev[PROF_STEPS], c.stream);
 		};
 		const uint32_t per_round = (flags ? 8u : 6u) + (fbits ? 4u : 0u);
-		// Rounds are replayed from a CUDA graph of ROUNDS_PER_GRAPH rounds; the
-		// host reads the control block once per replay. Rounds after the last
-		// one are no-ops.
-		constexpr uint32_t ROUNDS_PER_GRAPH = 16;
+		// Rounds are replayed from a CUDA graph of rpr rounds; the host reads
+		// the control block once per replay. Rounds after the last one are
+		// no-ops.
 		cudaGraph_t graph = nullptr;
 		cudaGraphExec_t exec = nullptr;
 		bool use_graph = !profile && cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
 		const uint32_t gcompact = grid_for(c, c.m, PEEL_THREADS / 32, 16);
-		// after every ROUNDS_PER_GRAPH rounds: the gated in-place compaction
+		// after every rpr rounds: the gated in-place compaction
+		const bool compaction = flags && compact_div != 0;
 		auto launch_compaction = [&]() {
-			if (!flags)
+			if (!compaction)
 				return;
 			k_compact_gate<<<1, 1, 0, c.stream>>>(ctl, T);
 			k_compact_spans<<<gcompact, PEEL_THREADS, 0, c.stream>>>(ctl, inc.span, c.m, inc.third, inc.tri,
 																	  inc.tpos);
 		};
-		const uint32_t per_replay = flags ? 2u : 0u;
+		const uint32_t per_replay = compaction ? 2u : 0u;
 		if (use_graph)
 		{
-			for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
+			for (uint32_t r = 0; r < rpr; ++r)
 				launch_round(nullptr, nullptr);
 			launch_compaction();
 			use_graph = cudaStreamEndCapture(c.stream, &graph) == cudaSuccess && graph &&
@@ -1360,12 +1386,12 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		uint32_t *trace_buf = nullptr; // (level, round, frontier size) per round
 		if (profile)
 		{
-			if (cudaMallocHost(&trace_buf, 3 * sizeof(uint32_t) * ROUNDS_PER_GRAPH) != cudaSuccess)
+			if (cudaMallocHost(&trace_buf, 3 * sizeof(uint32_t) * rpr) != cudaSuccess)
 			{
 				trace_buf = nullptr; // profile without the per-round lines
 				cudaGetLastError();
 			}
-			events.resize(size_t(ROUNDS_PER_GRAPH) * (PROF_STEPS + 1));
+			events.resize(size_t(rpr) * (PROF_STEPS + 1));
 			for (auto &e : events)
 				cudaEventCreate(&e);
 		}
@@ -1390,13 +1416,13 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			}
 			else
 			{
-				for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
+				for (uint32_t r = 0; r < rpr; ++r)
 					launch_round(profile ? &events[size_t(r) * (PROF_STEPS + 1)] : nullptr,
 								 trace_buf ? trace_buf + 3 * r : nullptr);
 				launch_compaction();
 			}
-			rounds += ROUNDS_PER_GRAPH;
-			c.launches += uint64_t(ROUNDS_PER_GRAPH) * per_round + per_replay;
+			rounds += rpr;
+			c.launches += uint64_t(rpr) * per_round + per_replay;
 			return cudaMemcpyAsync(&ring[slot], &ctl->c, sizeof(PeelCtl), cudaMemcpyDeviceToHost, c.stream) ==
 					   cudaSuccess &&
 				   cudaEventRecord(ring_ev[slot], c.stream) == cudaSuccess;
@@ -1422,7 +1448,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			++consumed;
 			if (profile)
 			{
-				for (uint32_t r = 0; r < ROUNDS_PER_GRAPH; ++r)
+				for (uint32_t r = 0; r < rpr; ++r)
 				{
 					const uint32_t *tr = trace_buf ? trace_buf + 3 * r : nullptr;
 					if (tr && !tr[2])

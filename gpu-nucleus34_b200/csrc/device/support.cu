@@ -50,8 +50,9 @@ __device__ __forceinline__ Lists tri_order(const uint32_t *__restrict__ tris, co
 // or binary search when the lists are very unequal). With WITH_OWN it also
 // counts the cliques whose lowest triangle id is t (the direct variant's
 // clique-list sizes); that needs the partner on the longest list too, found
-// by a forward-moving binary search.
-template <bool WITH_OWN>
+// by a forward-moving binary search. LANE_MAX is the shortest-list length up
+// to which a lane works alone (any value gives the same counts).
+template <uint32_t LANE_MAX, bool WITH_OWN>
 __global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__restrict__ tris, uint64_t T,
 															const uint2 *__restrict__ span,
 															const uint32_t *__restrict__ third,
@@ -70,7 +71,7 @@ __global__ void __launch_bounds__(SUP_THREADS, 4) k_support(const uint32_t *__re
 		Lists L{};
 		if (valid)
 			L = tri_order(tris, span, t);
-		const bool small = valid && L.a1 - L.a0 <= THREAD_MODE_MAX;
+		const bool small = valid && L.a1 - L.a0 <= LANE_MAX;
 		if (small)
 		{
 			uint32_t cnt = 0, mine = 0, lo_c = L.c0;
@@ -268,12 +269,19 @@ int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *tota
 			break;
 		}
 		const uint32_t grid = grid_for(c, (c.T + 31) / 32, SUP_THREADS / 32, 32);
-		if (own)
-			k_support<true><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.span, inc.third, inc.tri, support,
-																own, dtot);
+		static_assert(THREAD_MODE_MAX == TUNE_LANE_MAX, "default lane/warp split");
+		if (own) // the direct variant: default split
+			k_support<THREAD_MODE_MAX, true><<<grid, SUP_THREADS, 0, c.stream>>>(
+				c.dtris, c.T, inc.span, inc.third, inc.tri, support, own, dtot);
+		else if (c.tune.lane_max == 8)
+			k_support<8, false><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.span, inc.third, inc.tri,
+																	support, nullptr, dtot);
+		else if (c.tune.lane_max == 32)
+			k_support<32, false><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.span, inc.third, inc.tri,
+																	 support, nullptr, dtot);
 		else
-			k_support<false><<<grid, SUP_THREADS, 0, c.stream>>>(c.dtris, c.T, inc.span, inc.third, inc.tri,
-																 support, nullptr, dtot);
+			k_support<THREAD_MODE_MAX, false><<<grid, SUP_THREADS, 0, c.stream>>>(
+				c.dtris, c.T, inc.span, inc.third, inc.tri, support, nullptr, dtot);
 		c.launches++;
 		unsigned long long h = 0;
 		if (cudaGetLastError() != cudaSuccess ||

@@ -51,6 +51,8 @@ EXPORTED = (
     "nucleus34_strerror", "nucleus34_last_error",
     "nucleus34_ctx_create", "nucleus34_ctx_upload", "nucleus34_ctx_run",
     "nucleus34_ctx_copy_k", "nucleus34_ctx_destroy", "nucleus34_ctx_verify",
+    "nucleus34_tune_lookup", "nucleus34_tune_store", "nucleus34_ctx_set_tune", "nucleus34_ctx_last_tune",
+    "nucleus34_ctx_autotune",
     "nucleus34_graph_load", "nucleus34_graph_from_edges", "nucleus34_graph_save_grh",
     "nucleus34_graph_release", "nucleus34_graph_csr",
     "nucleus34_gen_rmat", "nucleus34_gen_rgg", "nucleus34_gen_ws",
@@ -75,6 +77,25 @@ class Csr(C.Structure):
 class Opts(C.Structure):
     _fields_ = [("mem_budget_bytes", C.c_uint64), ("device", C.c_int),
                 ("parts", C.c_uint32), ("tune_table", C.c_char_p), ("flags", C.c_uint32)]
+
+
+TUNE_NEVER = 0xFFFFFFFF
+_TUNE_FIELDS = ("lane_max", "compact_div", "sort_shift", "rounds_per_replay")
+
+
+class Tune(C.Structure):
+    """nucleus34_tune: scheduling settings of the on-demand variant (0 = default)."""
+    _fields_ = [(f, C.c_uint32) for f in _TUNE_FIELDS]
+
+    def as_dict(self) -> dict:
+        return {f: ("never" if getattr(self, f) == TUNE_NEVER else int(getattr(self, f))) for f in _TUNE_FIELDS}
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "Tune":
+        unknown = set(d) - set(_TUNE_FIELDS)
+        if unknown:
+            raise ValueError(f"unknown tune settings: {sorted(unknown)}")
+        return cls(*[TUNE_NEVER if d.get(f, 0) == "never" else int(d.get(f, 0)) for f in _TUNE_FIELDS])
 
 
 class Result(C.Structure):
@@ -209,6 +230,18 @@ def lib() -> C.CDLL:
     L.nucleus34_ctx_verify.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.nucleus34_ctx_verify.restype = C.c_int
     L.nucleus34_ctx_destroy.argtypes = [C.c_void_p]
+    L.nucleus34_tune_lookup.argtypes = [C.c_char_p, u64, u64, u64, C.c_uint32, C.POINTER(Tune), C.POINTER(C.c_int)]
+    L.nucleus34_tune_lookup.restype = C.c_int
+    L.nucleus34_tune_store.argtypes = [C.c_char_p, u64, u64, u64, C.c_uint32, C.POINTER(Tune), C.c_double,
+                                       C.c_double]
+    L.nucleus34_tune_store.restype = C.c_int
+    L.nucleus34_ctx_set_tune.argtypes = [C.c_void_p, C.POINTER(Tune)]
+    L.nucleus34_ctx_set_tune.restype = C.c_int
+    L.nucleus34_ctx_last_tune.argtypes = [C.c_void_p, C.POINTER(Tune)]
+    L.nucleus34_ctx_last_tune.restype = C.c_int
+    L.nucleus34_ctx_autotune.argtypes = [C.c_void_p, C.c_char_p, C.POINTER(Tune), C.POINTER(C.c_double),
+                                         C.POINTER(C.c_double)]
+    L.nucleus34_ctx_autotune.restype = C.c_int
     L.nucleus34_ctx_destroy.restype = None
     L.nucleus34_graph_load.argtypes = [C.c_char_p, C.POINTER(Graph)]
     L.nucleus34_graph_load.restype = C.c_int
@@ -352,16 +385,37 @@ OPT_LEAN_MEMORY = 0x4
 OPT_VERIFIABLE = 0x8
 
 
-def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1, flags: int = 0) -> Opts:
-    return Opts(mem_budget_bytes, device, parts, None, flags)
+def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1, flags: int = 0,
+              tune_table: Optional[str] = None) -> Opts:
+    return Opts(mem_budget_bytes, device, parts, os.fsencode(tune_table) if tune_table else None, flags)
+
+
+def tune_lookup(path: str, triangles: int, n: int, m: int, max_out: int) -> tuple:
+    """(settings dict, matched) that the tune table at path gives a graph of
+    `triangles` triangles whose oriented CSR has n vertices, m edges and
+    maximum out-degree max_out (nucleus34_tune_lookup; host only)."""
+    t, matched = Tune(), C.c_int()
+    _check(lib().nucleus34_tune_lookup(os.fsencode(path), triangles, n, m, max_out, C.byref(t),
+                                       C.byref(matched)), "tune_lookup")
+    return t.as_dict(), bool(matched.value)
+
+
+def tune_store(path: str, triangles: int, n: int, m: int, max_out: int, settings: dict,
+               sec: float = 0.0, default_sec: float = 0.0) -> None:
+    """Writes settings as the line of that graph's class into the table at
+    path (nucleus34_tune_store; host only)."""
+    t = Tune.from_dict(settings)
+    _check(lib().nucleus34_tune_store(os.fsencode(path), triangles, n, m, max_out, C.byref(t), sec, default_sec),
+           "tune_store")
 
 
 def decompose(g: HostGraph, variant="direct", device: int = 0, mem_budget_bytes: int = 0,
-              n_quds: int = 5, kfile: Optional[str] = None, flags: int = 0) -> Decomposition:
+              n_quds: int = 5, kfile: Optional[str] = None, flags: int = 0,
+              tune_table: Optional[str] = None) -> Decomposition:
     """One-shot decomposition through nucleus34_decompose[_ondemand]."""
     L = lib()
     v = _VARIANTS[variant]
-    opts = make_opts(device, mem_budget_bytes, flags=flags)
+    opts = make_opts(device, mem_budget_bytes, flags=flags, tune_table=tune_table)
     res = Result()
     h = C.c_void_p()
     csr = g.csr()
@@ -505,9 +559,10 @@ class Server:
 class Context:
     """Device-resident context: upload once, run many times."""
 
-    def __init__(self, device: int = 0, mem_budget_bytes: int = 0, flags: int = 0):
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0, flags: int = 0,
+                 tune_table: Optional[str] = None):
         self._L = lib()
-        self._opts = make_opts(device, mem_budget_bytes, flags=flags)
+        self._opts = make_opts(device, mem_budget_bytes, flags=flags, tune_table=tune_table)
         self._h = C.c_void_p()
         _check(self._L.nucleus34_ctx_create(C.byref(self._opts), C.byref(self._h)), "ctx_create")
 
@@ -528,6 +583,24 @@ class Context:
             self._h, k.ctypes.data_as(C.POINTER(C.c_int32)),
             _u32p(tris) if tris is not None else None), "ctx_copy_k")
         return (k, tris.reshape(-1, 3)) if with_tris else k
+
+    def set_tune(self, settings: Optional[dict]) -> None:
+        """Pins the on-demand settings of later runs (None: back to the table / defaults)."""
+        t = Tune.from_dict(settings) if settings is not None else None
+        _check(self._L.nucleus34_ctx_set_tune(self._h, C.byref(t) if t is not None else None), "ctx_set_tune")
+
+    def last_tune(self) -> dict:
+        t = Tune()
+        _check(self._L.nucleus34_ctx_last_tune(self._h, C.byref(t)), "ctx_last_tune")
+        return t.as_dict()
+
+    def autotune(self, table: Optional[str] = None) -> dict:
+        """nucleus34_ctx_autotune on the uploaded graph: the best settings and
+        the device times (s) of the default and the tuned decomposition."""
+        t, best, default = Tune(), C.c_double(), C.c_double()
+        _check(self._L.nucleus34_ctx_autotune(self._h, os.fsencode(table) if table else None, C.byref(t),
+                                              C.byref(best), C.byref(default)), "ctx_autotune")
+        return {"tune": t.as_dict(), "tuned_sec": best.value, "default_sec": default.value}
 
     def verify(self) -> tuple:
         """(violations, checked) of nucleus34_ctx_verify for the last run."""

@@ -70,7 +70,8 @@ typedef struct
 	uint64_t mem_budget_bytes; /* 0 = 90% of the device's free memory */
 	int device;                /* CUDA ordinal */
 	uint32_t parts;            /* accepted for CLI parity (cuNucleus34.cu:161-169); one GPU */
-	const char *tune_table;    /* optional autotune table path, NULL = built-in defaults */
+	const char *tune_table;    /* tune table path (see nucleus34_tune below), read and checked when
+	                              the context is created; NULL = built-in defaults */
 	uint32_t flags;            /* NUCLEUS34_OPT_* bits, 0 = defaults */
 } nucleus34_opts;
 
@@ -181,6 +182,68 @@ void nucleus34_ctx_destroy(nucleus34_ctx ctx);
  * receives the number of triangles (and rounds) that fail; *checked the
  * number of triangles examined. Rebuilds the edge->triangle incidence. */
 int nucleus34_ctx_verify(nucleus34_ctx ctx, uint64_t *violations, uint64_t *checked);
+
+/* ---- tuning (scheduling settings of the on-demand variant) -------------- */
+
+/* Every setting gives bit-identical results: a setting only moves a
+ * triangle between the lane and warp kernels, or changes when the incidence
+ * is compacted, when a frontier is put in id order and how many peel rounds
+ * one CUDA graph replay holds. A zero field means the built-in default. The
+ * direct variant always runs with the defaults. */
+#define NUCLEUS34_TUNE_NEVER 0xffffffffu
+typedef struct
+{
+	uint32_t lane_max;          /* shortest-list length up to which one lane rather than a warp
+	                               takes a triangle (support count and peel): 8, 16 (default), 32 */
+	uint32_t compact_div;       /* compact the incidence once the triangles peeled since the last
+	                               compaction reach 1/compact_div of the live ones: 1..64
+	                               (default 8), or NUCLEUS34_TUNE_NEVER */
+	uint32_t sort_shift;        /* put a frontier of at least max(T >> sort_shift, 4096) triangles
+	                               in id order: 1..31 (default 12), or NUCLEUS34_TUNE_NEVER */
+	uint32_t rounds_per_replay; /* peel rounds per CUDA graph replay: 1..64 (default 16) */
+} nucleus34_tune;
+
+/* A tune table is a text file of lines
+ *     size=<s> skew=<w> [lane_max=..] [compact_div=..|never] [sort_shift=..|never]
+ *     [rounds_per_replay=..] [sec=..] [default_sec=..]
+ * ('#' starts a comment). A graph's class is size = floor(log2 T) and
+ * skew = floor(log2(max out-degree * n / m)) of its degree-oriented CSR
+ * (0 when m = 0). A run takes the line of its skew class whose size is
+ * nearest, if within 2 (ties to the earlier line); otherwise the defaults.
+ * sec and default_sec record the autotuner's timings and are not used. */
+
+/* The settings that the table at path gives a graph of `triangles`
+ * triangles whose oriented CSR has n vertices, m edges and maximum
+ * out-degree max_out; defaults filled in. *matched (if non-NULL) = 1 when a
+ * line applied. E_IO: unreadable; E_INVALID: a malformed line (the detail
+ * names it). */
+int nucleus34_tune_lookup(const char *path, uint64_t triangles, uint64_t n, uint64_t m, uint32_t max_out,
+						  nucleus34_tune *out, int *matched);
+/* Writes `tune` (defaults filled in) as the line of that graph's class into
+ * the table at path, replacing a line of the same class or appending one
+ * (the file is created when missing and rewritten through a temporary and a
+ * rename; a table that does not parse is left alone: E_INVALID). sec and
+ * default_sec are recorded as given. */
+int nucleus34_tune_store(const char *path, uint64_t triangles, uint64_t n, uint64_t m, uint32_t max_out,
+						 const nucleus34_tune *tune, double sec, double default_sec);
+/* Pins the settings of the context's later on-demand runs (NULL: back to
+ * its tune table, or the defaults). E_INVALID for a value out of range. */
+int nucleus34_ctx_set_tune(nucleus34_ctx ctx, const nucleus34_tune *tune);
+/* The settings the last run used, defaults filled in. */
+int nucleus34_ctx_last_tune(nucleus34_ctx ctx, nucleus34_tune *out);
+/* Autotuner for the uploaded graph: times its on-demand decomposition under
+ * the defaults, then under candidate settings, one field at a time (each
+ * field keeps the best value found before the next is tried; a candidate
+ * must beat the best so far by 1% twice). Every run's k must equal the
+ * default run's bit for bit (E_CUDA otherwise). The best settings go to
+ * *best, their time and the default time (s, device-timed t_total) to
+ * *best_sec and *default_sec, and, when path is non-NULL, into the table
+ * at path as the line of this graph's class (a line of the same class is
+ * replaced; the file is rewritten through a temporary and a rename).
+ * Needs host memory for two copies of k (8 bytes per triangle). The
+ * context's pinned settings are restored afterwards. */
+int nucleus34_ctx_autotune(nucleus34_ctx ctx, const char *path, nucleus34_tune *best, double *best_sec,
+						   double *default_sec);
 
 /* ---- batched decomposition ------------------------------------------------ */
 
