@@ -54,7 +54,9 @@ __device__ __forceinline__ Lists order_lists(uint32_t x0, uint32_t x1, uint32_t 
 	return Lists{p0, p1, q0, q1, r0, r1};
 }
 
-// Shortest-list length up to which one lane handles a triangle on its own.
+// Shortest-list length up to which one lane handles a triangle on its own
+// (the default; the on-demand variant's scheduling settings instantiate the
+// support count and the peel debit with 8, 16 or 32).
 constexpr uint32_t THREAD_MODE_MAX = 16;
 // B longer than this multiple of A: binary-search B instead of merging.
 constexpr uint32_t MERGE_RATIO = 24;

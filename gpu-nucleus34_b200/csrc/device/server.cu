@@ -295,6 +295,7 @@ int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_o
 		return fail(NUCLEUS34_E_OOM_BUDGET, "host allocation failed");
 	if (opts)
 		s->opts = *opts;
+	s->opts.tune_table = nullptr; // read by each worker context as it is created; not kept
 	const uint32_t nw = (sopts && sopts->workers) ? sopts->workers : 2u;
 	s->max_batch = (sopts && sopts->max_batch_graphs) ? sopts->max_batch_graphs : 256;
 	for (uint32_t i = 0; i < nw; ++i)

@@ -448,7 +448,7 @@ int load_graph(const char *path, HostGraph &g)
 	// Each chunk parses into its own uninitialised buffers, sized for the
 	// most pair lines it can hold (a pair line has at least 4 characters,
 	// "1 2\n"). The two numbers are read in one pass from the line start
-	// (parse_two stops at the first character that is neither a digit, a
+	// (parse_two_at stops at the first character that is neither a digit, a
 	// space nor a tab, so the bound is the chunk end), then the rest of the
 	// line is skipped.
 	std::vector<std::unique_ptr<uint32_t[]>> ps(nchunks), pd(nchunks);
