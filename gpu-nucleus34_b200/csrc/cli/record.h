@@ -304,10 +304,17 @@ struct Error
 	std::string msg;
 };
 
+// The record's "error" is the exception text the reference would print
+// (e.what(), cuNucleus34_ondemand.cu:762-778): the library's detail message,
+// which repeats the reference's texts for reader errors ("Dataset <f> is not
+// accessible!", "Unknown dataset format: <ext>", ...); the call and status
+// name only when there is no detail.
 inline void check(int rc, const char *what)
 {
-	if (rc != NUCLEUS34_OK)
-		throw Error{rc, std::string(what) + ": " + nucleus34_strerror(rc) + " (" + nucleus34_last_error() + ")"};
+	if (rc == NUCLEUS34_OK)
+		return;
+	const std::string detail = nucleus34_last_error();
+	throw Error{rc, detail.empty() ? std::string(what) + ": " + nucleus34_strerror(rc) : detail};
 }
 
 } // namespace rec
