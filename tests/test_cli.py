@@ -19,6 +19,21 @@ PROGRAMS = ["cuNucleus34", "cuNucleus34_ondemand"]
 K4_TEXT = "% comment\n1 2\n1 2\n2 3\n1 3\n3 4\n1 4\n2 4\n"
 
 
+# dataset keys of a complete record, in the reference's order
+# (cuNucleus34.cu:229-795, cuNucleus34_ondemand.cu field calls)
+KEYS = {
+    "cuNucleus34": ["file", "vertex_count", "edge_count", "data_loading_time_sec", "data_memory_bytes",
+                    "triangle_time_sec", "triangle_count", "triangles", "triangle_graph_time_sec",
+                    "four_clique_time_sec", "four_clique_count", "four-cliques", "four_clique_graph_time_sec",
+                    "peeling_mode", "peeling_preprocess_time_sec", "peeling_time_sec", "peeling_iterations",
+                    "K_max", "total_time_sec", "K_count", "K", "K_avg"],
+    "cuNucleus34_ondemand": ["file", "vertex_count", "edge_count", "data_loading_time_sec", "triangle_time_sec",
+                             "triangle_count", "incidence_time_sec", "incidence_entries", "four_clique_time_sec",
+                             "four_clique_count", "unpeeled_count", "peeling_mode", "peeling_time_sec",
+                             "peeling_iterations", "K_max", "total_time_sec", "K_count", "K", "K_avg"],
+}
+
+
 def run(prog, *args):
     r = subprocess.run([os.path.join(BIN, prog), *map(str, args)], capture_output=True, text=True, timeout=300)
     return r.returncode, r.stdout, r.stderr
@@ -87,6 +102,7 @@ def test_records_and_k_files_match_the_oracle(n34, oracle, prog, tmp_path):
     assert rc == 0, err
     ds = record(out)["dataset"]
     assert "error" not in ds, ds.get("error")
+    assert list(ds) == KEYS[prog]
     assert ds["vertex_count"] == g.n and ds["edge_count"] == 2 * g.m
     assert ds["triangle_count"] == want.T and ds["four_clique_count"] == want.Q
     assert ds["K_max"] == want.k_max and ds["K_count"] == want.T
