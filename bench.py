@@ -148,8 +148,9 @@ def measured_peaks():
         return PEAKS_FALLBACK, "fallback"
 
 
-def cpu_reference_run(a, steps: int):
-    """Times the reference's CPU path (or the oracle port) on the bounded sample."""
+def cpu_reference_run(a, steps: int, warmup: int = 0):
+    """Times the reference's CPU path (or the oracle port) on the bounded
+    sample: `warmup` untimed runs, then `steps` timed ones (median)."""
     import nucleus34 as n34
     ref = os.path.join(ROOT, "oracle", "_ref", "cpu_ref")
     kind = "reference"
@@ -162,6 +163,8 @@ def cpu_reference_run(a, steps: int):
         path = os.path.join(td, "sample.edges")
         s, d = n34.gen_rmat(a.cpu_sample_scale, a.edge_factor, a.seed)
         n34.write_edges(s, d, path)
+        for _ in range(warmup):
+            subprocess.run([ref, path], check=True, capture_output=True, text=True)
         vals, recs = [], []
         for _ in range(steps):
             out = subprocess.run([ref, path], check=True, capture_output=True, text=True).stdout
@@ -415,10 +418,11 @@ def main():
         if rank != 0:
             return 0
         steps = max(1, a.steps)
-        cb = cpu_reference_run(a, steps)
+        warmup = max(0, a.warmup)
+        cb = cpu_reference_run(a, steps, warmup)
         line = {
             "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": a.gpus,
-            "steps": steps, "warmup": 0, "ms_per_step": cb["t_decomp_s"] * 1e3, "higher_is_better": True,
+            "steps": steps, "warmup": warmup, "ms_per_step": cb["t_decomp_s"] * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32", "data": "synthetic",
             "config": {"workload": workload_name(a), "sample": cb["sample"]},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},

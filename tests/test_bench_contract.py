@@ -1,0 +1,46 @@
+"""bench.py's reference arm (the reference's CPU path on a bounded sample of
+the workload), run here on the CPU: one JSON line with the contract's keys;
+under several ranks only rank 0 runs and prints."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def run_bench(*args, env=None):
+    e = dict(os.environ)
+    e.update(env or {})
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), *map(str, args)], capture_output=True,
+                       text=True, timeout=600, env=e, cwd=ROOT)
+    return r.returncode, r.stdout, r.stderr
+
+
+def test_reference_arm_prints_one_contract_line():
+    rc, out, err = run_bench("--impl", "reference", "--steps", 2, "--warmup", 1, "--cpu-sample-scale", 10)
+    assert rc == 0, err
+    lines = [l for l in out.splitlines() if l.strip()]
+    assert len(lines) == 1
+    j = json.loads(lines[0])
+    assert j["impl"] == "reference"
+    assert j["metric"] == "triangles peeled/sec" and j["unit"] == "triangles/s"
+    assert j["higher_is_better"] is True and j["scaling"] == "weak"
+    assert j["steps"] == 2 and j["warmup"] == 1 and j["n_gpus"] == 1
+    assert j["value"] > 0 and j["ms_per_step"] > 0
+    assert j["vs_baseline"] is None and j["data"] == "synthetic"
+    assert j["config"]["workload"].startswith("R-MAT scale 20 ef 16")
+    cb = j["cpu_baseline"]
+    assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1
+    assert cb["value"] == j["value"] and cb["unit"] == j["unit"]
+    assert "R-MAT scale 10" in cb["sample"]
+    assert j["e2e"] == {"value": j["value"], "unit": j["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_runs_on_rank_zero_only():
+    rc, out, err = run_bench("--impl", "reference", "--gpus", 2, "--steps", 1, "--warmup", 0,
+                             "--cpu-sample-scale", 10, env={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
+    assert rc == 0, err
+    assert out.strip() == ""
