@@ -18,6 +18,12 @@ CASES = [
     {"name": "quirks_txt", "kind": "text", "ext": ".txt"},
     {"name": "quirks_mtx3", "kind": "mtx3", "ext": ".mtx"},
     {"name": "quirks_mtx2", "kind": "mtx2", "ext": ".mtx"},
+    {"name": "rmat13_ef24_s99", "kind": "rmat", "scale": 13, "ef": 24, "seed": 99, "ext": ".edges"},
+    {"name": "ws5000_k16_b03_s21", "kind": "ws", "n": 5000, "k": 16, "beta": 0.3, "seed": 21, "ext": ".edges"},
+    {"name": "rgg40000_d40_s8", "kind": "rgg", "n": 40000, "deg": 40.0, "seed": 8, "ext": ".edges"},
+    {"name": "hubs3000_s2", "kind": "hubs", "n": 3000, "seed": 2, "ext": ".edges"},
+    {"name": "cliques4to14", "kind": "cliques", "seed": 5, "ext": ".txt"},
+    {"name": "k8_chain40_s6", "kind": "chain", "links": 40, "seed": 6, "ext": ".edges"},
 ]
 
 QUIRKS_TXT = """# a comment line
@@ -78,6 +84,54 @@ QUIRKS_MTX2 = """%%MatrixMarket
 """
 
 
+def structured_pairs(case):
+    """Seeded structured graphs (undirected pairs, possibly repeated):
+    hubs: three hubs joined to every vertex, a dense 150-vertex core and
+      sparse random edges (long, skewed incidence lists);
+    cliques: disjoint K4..K14 joined by single bridge edges (k = n - 3 inside
+      each clique);
+    chain: K8s in a row, each sharing three vertices (a triangle) with the
+      next, plus a few random chords."""
+    rng = np.random.default_rng(case["seed"])
+    kind = case["kind"]
+    pairs = []
+    if kind == "hubs":
+        n = case["n"]
+        for h in range(3):
+            pairs += [(h, v) for v in range(3, n)]
+        core = np.arange(3, 153)
+        for i in range(len(core)):
+            for j in range(i + 1, len(core)):
+                if rng.random() < 0.3:
+                    pairs.append((int(core[i]), int(core[j])))
+        a = rng.integers(3, n, 6 * n)
+        b = rng.integers(3, n, 6 * n)
+        pairs += list(zip(a.tolist(), b.tolist()))
+    elif kind == "cliques":
+        base = 0
+        prev = None
+        for size in range(4, 15):
+            vs = list(range(base, base + size))
+            pairs += [(u, v) for i, u in enumerate(vs) for v in vs[i + 1:]]
+            if prev is not None:
+                pairs.append((prev, vs[int(rng.integers(0, size))]))
+            prev = vs[-1]
+            base += size
+    else:  # chain
+        step = 5  # 8 vertices per clique, 3 shared with the next
+        for c in range(case["links"]):
+            vs = list(range(c * step, c * step + 8))
+            pairs += [(u, v) for i, u in enumerate(vs) for v in vs[i + 1:]]
+        top = case["links"] * step + 3
+        a = rng.integers(0, top, 30)
+        b = rng.integers(0, top, 30)
+        pairs += list(zip(a.tolist(), b.tolist()))
+    perm = rng.permutation(len(pairs))
+    src = np.array([pairs[i][0] for i in perm], np.uint32)
+    dst = np.array([pairs[i][1] for i in perm], np.uint32)
+    return src, dst
+
+
 def materialise(case, directory):
     """Writes the case's input file into `directory` and returns its path."""
     import nucleus34
@@ -94,6 +148,9 @@ def materialise(case, directory):
             nucleus34.save_grh(nucleus34.graph_from_edges(s, d), path)
         else:
             nucleus34.write_edges(s, d, path)
+    elif kind in ("hubs", "cliques", "chain"):
+        s, d = structured_pairs(case)
+        nucleus34.write_edges(s, d, path)
     else:
         text = {"text": QUIRKS_TXT, "mtx3": QUIRKS_MTX3, "mtx2": QUIRKS_MTX2}[kind]
         with open(path, "w") as f:

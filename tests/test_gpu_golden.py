@@ -1,6 +1,6 @@
 """The CUDA path against the golden fixtures themselves: the outputs of the
 reference's own host code (tests/golden/make_golden.py runs
-oracle/_ref/cpu_ref) on the nine golden inputs. Both variants, through the
+oracle/_ref/cpu_ref) on every golden input. Both variants, through the
 C-ABI: counts, K_max, K_avg to the 6 significant digits the reference prints,
 and the k file byte for byte (sha256)."""
 import hashlib
