@@ -189,7 +189,9 @@ int nucleus34_ctx_verify(nucleus34_ctx ctx, uint64_t *violations, uint64_t *chec
  * triangle between the lane and warp kernels, or changes when the incidence
  * is compacted, when a frontier is put in id order and how many peel rounds
  * one CUDA graph replay holds. A zero field means the built-in default. The
- * direct variant always runs with the defaults. */
+ * direct variant always runs with the defaults. No reference counterpart:
+ * the reference's kernels run with fixed launch shapes and one peel round per
+ * host iteration (cuNucleus34_ondemand.cu:599-682). */
 #define NUCLEUS34_TUNE_NEVER 0xffffffffu
 typedef struct
 {
