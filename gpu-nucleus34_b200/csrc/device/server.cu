@@ -205,18 +205,17 @@ void worker_loop(nucleus34_server_s *s, size_t wi)
 		{
 			std::unique_lock<std::mutex> lk(s->mu);
 			s->cv_work.wait(lk, [&] {
-				if (s->stop)
-					return true;
 				if (s->pending.empty())
-					return false;
-				// the head fits the memory left, or nothing else is running
+					return s->stop;
+				// the head fits the memory left, or nothing else is running;
+				// while stopping too, so that the queued requests are finished
+				// under the same budget (a running pass always ends and wakes
+				// the waiting workers)
 				const uint64_t free_b = s->budget > s->in_flight_bytes ? s->budget - s->in_flight_bytes : 0;
 				return s->pending.front()->est_bytes <= free_b || s->in_flight_bytes == 0;
 			});
-			if (s->stop && s->pending.empty())
-				return;
 			if (s->pending.empty())
-				continue;
+				return; // stopping, nothing queued
 			uint64_t free_b = s->budget > s->in_flight_bytes ? s->budget - s->in_flight_bytes : 0;
 			// admission in arrival order: the head always (it fits, or runs
 			// alone on an idle device), then followers while they fit
