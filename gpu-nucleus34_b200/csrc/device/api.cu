@@ -739,6 +739,46 @@ int nucleus34_ctx_copy_k(nucleus34_ctx ctx, int32_t *k_out, uint32_t *tris_out)
 
 void nucleus34_ctx_destroy(nucleus34_ctx ctx) { destroy_ctx(ctx); }
 
+int nucleus34_ctx_upload_edges(nucleus34_ctx ctx, const uint32_t *src, const uint32_t *dst, uint64_t count,
+							   uint64_t *n_out, uint64_t *m_out)
+{
+	if (!ctx)
+		return fail(NUCLEUS34_E_INVALID, "null context");
+	return guarded([&]() -> int {
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		N34_TRY(upload_edges(ctx->c, src, dst, count));
+		if (n_out)
+			*n_out = ctx->c.n;
+		if (m_out)
+			*m_out = ctx->c.m;
+		return NUCLEUS34_OK;
+	});
+}
+
+int nucleus34_ctx_copy_csr(nucleus34_ctx ctx, uint32_t *O, uint32_t *D, uint32_t *E)
+{
+	if (!ctx)
+		return fail(NUCLEUS34_E_INVALID, "null context");
+	return guarded([&]() -> int {
+		std::lock_guard<std::mutex> lk(ctx->c.mu);
+		Ctx &c = ctx->c;
+		if (!c.dO)
+			return fail(NUCLEUS34_E_STATE, "no graph uploaded");
+		N34_TRY(set_device(c));
+		std::vector<uint32_t> h(c.n + 1);
+		N34_CUDA(cudaMemcpyAsync(h.data(), c.dO, (c.n + 1) * 4, cudaMemcpyDeviceToHost, c.stream));
+		if (E && c.m)
+			N34_CUDA(cudaMemcpyAsync(E, c.dE, c.m * 4, cudaMemcpyDeviceToHost, c.stream));
+		N34_CUDA(cudaStreamSynchronize(c.stream));
+		if (O)
+			std::copy(h.begin(), h.end(), O);
+		if (D)
+			for (uint64_t u = 0; u < c.n; ++u)
+				D[u] = h[u + 1] - h[u];
+		return NUCLEUS34_OK;
+	});
+}
+
 int nucleus34_ctx_set_tune(nucleus34_ctx ctx, const nucleus34_tune *tune)
 {
 	if (!ctx)

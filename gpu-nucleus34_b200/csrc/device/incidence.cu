@@ -418,6 +418,81 @@ int build_incidence(Ctx &c, Incidence &inc, bool want_tpos, bool lean)
 	return rc;
 }
 
+// The segmented sort above for other builders: every segment
+// [off[s], off[s+1]) of keys (nseg < 2^32 segments) ascending, with the same
+// three size classes and kernels as the incidence build.
+int sort_segments_u64(Ctx &c, unsigned long long *keys, const uint64_t *off, uint64_t nseg)
+{
+	if (nseg == 0)
+		return NUCLEUS34_OK;
+	if (nseg > 0xffffffffull)
+		return fail(NUCLEUS34_E_RANGE32, "segment count exceeds 32-bit segment ids");
+	uint32_t *lists = nullptr, *counts = nullptr;
+	unsigned long long *scratch = nullptr, *maxlen = nullptr;
+	int rc = NUCLEUS34_OK;
+	const EntryStore store{keys, nullptr, nullptr};
+	do
+	{
+		if ((rc = dalloc(c, &lists, 3 * nseg, "segment lists")) || (rc = dalloc(c, &counts, 4, "segment counts")) ||
+			(rc = dalloc(c, &maxlen, 1, "segment max")))
+			break;
+		if (cudaMemsetAsync(counts, 0, 16, c.stream) != cudaSuccess ||
+			cudaMemsetAsync(maxlen, 0, 8, c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "memset");
+			break;
+		}
+		k_seg_classify<<<grid_for(c, nseg, 256), 256, 0, c.stream>>>(off, nseg, lists, counts, nseg, maxlen);
+		c.launches++;
+		uint32_t hcounts[4] = {0, 0, 0, 0};
+		unsigned long long hmax = 0;
+		if (cudaMemcpyAsync(hcounts, counts, 16, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaMemcpyAsync(&hmax, maxlen, 8, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
+			cudaStreamSynchronize(c.stream) != cudaSuccess)
+		{
+			rc = fail(NUCLEUS34_E_CUDA, "segment classify");
+			break;
+		}
+		if (hcounts[0])
+		{
+			k_seg_sort_warp<<<grid_for(c, hcounts[0], 8, 32), 256, 0, c.stream>>>(lists, counts + 0, off, store);
+			c.launches++;
+		}
+		if (hcounts[1])
+		{
+			const size_t smem = SEG_SMEM * sizeof(unsigned long long);
+			cudaFuncSetAttribute(k_seg_sort_block, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+			k_seg_sort_block<<<grid_for(c, hcounts[1], 1, 2), SEG_BLOCK, smem, c.stream>>>(lists + nseg,
+																							counts + 1, off, store);
+			c.launches++;
+		}
+		if (hcounts[2])
+		{
+			uint64_t P = 64;
+			while (P < hmax)
+				P <<= 1;
+			if (P > 0xffffffffull)
+			{
+				rc = fail(NUCLEUS34_E_RANGE32, "segment longer than the sort's 32-bit index range");
+				break;
+			}
+			const uint32_t blocks = std::min<uint32_t>(hcounts[2], uint32_t(c.sm_count));
+			if ((rc = dalloc(c, &scratch, P * blocks, "segment sort scratch")))
+				break;
+			k_seg_sort_global<<<blocks, SEG_BLOCK, 0, c.stream>>>(lists + 2 * nseg, counts + 2, off, store, scratch,
+																  P);
+			c.launches++;
+		}
+		if (cudaGetLastError() != cudaSuccess)
+			rc = fail(NUCLEUS34_E_CUDA, "segment sort kernels");
+	} while (false);
+	c.release(lists);
+	c.release(counts);
+	c.release(maxlen);
+	c.release(scratch);
+	return rc;
+}
+
 void free_incidence(Ctx &c, Incidence &inc)
 {
 	c.release(inc.span);

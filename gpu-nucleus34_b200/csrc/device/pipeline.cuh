@@ -41,6 +41,12 @@ int list_triangles(Ctx &c);
 // lean: no 64-bit key array (entries sorted in place as pairs) and no tpos.
 int build_incidence(Ctx &c, Incidence &inc, bool want_tpos, bool lean = false);
 void free_incidence(Ctx &c, Incidence &inc);
+// Sorts every segment [off[s], off[s+1]) of keys ascending (incidence.cu's
+// segmented sort; nseg < 2^32).
+int sort_segments_u64(Ctx &c, unsigned long long *keys, const uint64_t *off, uint64_t nseg);
+// Oriented CSR of an edge list built on the device and made resident in c
+// (csr_build.cu), with the host build's semantics.
+int upload_edges(Ctx &c, const uint32_t *src, const uint32_t *dst, uint64_t count);
 // support[t] = number of four-cliques on t; returns sum(support) in *total.
 // own (optional): cliques whose lowest triangle is t (direct variant sizes).
 int count_support(Ctx &c, const Incidence &inc, int32_t *support, uint64_t *total, uint32_t *own);

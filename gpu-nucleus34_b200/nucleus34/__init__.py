@@ -52,7 +52,7 @@ EXPORTED = (
     "nucleus34_ctx_create", "nucleus34_ctx_upload", "nucleus34_ctx_run",
     "nucleus34_ctx_copy_k", "nucleus34_ctx_destroy", "nucleus34_ctx_verify",
     "nucleus34_tune_lookup", "nucleus34_tune_store", "nucleus34_ctx_set_tune", "nucleus34_ctx_last_tune",
-    "nucleus34_ctx_autotune",
+    "nucleus34_ctx_autotune", "nucleus34_ctx_upload_edges", "nucleus34_ctx_copy_csr",
     "nucleus34_graph_load", "nucleus34_graph_from_edges", "nucleus34_graph_save_grh",
     "nucleus34_graph_release", "nucleus34_graph_csr",
     "nucleus34_gen_rmat", "nucleus34_gen_rgg", "nucleus34_gen_ws",
@@ -230,6 +230,11 @@ def lib() -> C.CDLL:
     L.nucleus34_ctx_verify.argtypes = [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
     L.nucleus34_ctx_verify.restype = C.c_int
     L.nucleus34_ctx_destroy.argtypes = [C.c_void_p]
+    L.nucleus34_ctx_upload_edges.argtypes = [C.c_void_p, u32p, u32p, u64, C.POINTER(C.c_uint64),
+                                             C.POINTER(C.c_uint64)]
+    L.nucleus34_ctx_upload_edges.restype = C.c_int
+    L.nucleus34_ctx_copy_csr.argtypes = [C.c_void_p, u32p, u32p, u32p]
+    L.nucleus34_ctx_copy_csr.restype = C.c_int
     L.nucleus34_tune_lookup.argtypes = [C.c_char_p, u64, u64, u64, C.c_uint32, C.POINTER(Tune), C.POINTER(C.c_int)]
     L.nucleus34_tune_lookup.restype = C.c_int
     L.nucleus34_tune_store.argtypes = [C.c_char_p, u64, u64, u64, C.c_uint32, C.POINTER(Tune), C.c_double,
@@ -564,11 +569,35 @@ class Context:
         self._L = lib()
         self._opts = make_opts(device, mem_budget_bytes, flags=flags, tune_table=tune_table)
         self._h = C.c_void_p()
+        self._nm = (0, 0)  # (n, m) of the resident graph
         _check(self._L.nucleus34_ctx_create(C.byref(self._opts), C.byref(self._h)), "ctx_create")
 
     def upload(self, g: HostGraph) -> None:
         csr = g.csr()
         _check(self._L.nucleus34_ctx_upload(self._h, C.byref(csr)), "ctx_upload")
+        self._nm = (int(g.n), int(g.m))
+
+    def upload_edges(self, src: np.ndarray, dst: np.ndarray) -> tuple:
+        """nucleus34_ctx_upload_edges: the oriented CSR of an edge list built on
+        the device (graph_from_edges semantics); returns (n, m)."""
+        src = np.ascontiguousarray(src, np.uint32)
+        dst = np.ascontiguousarray(dst, np.uint32)
+        if len(src) != len(dst):
+            raise ValueError("src and dst differ in length")
+        n, m = C.c_uint64(), C.c_uint64()
+        _check(self._L.nucleus34_ctx_upload_edges(self._h, _u32p(src), _u32p(dst), len(src), C.byref(n),
+                                                  C.byref(m)), "ctx_upload_edges")
+        self._nm = (int(n.value), int(m.value))
+        return self._nm
+
+    def copy_csr(self) -> "HostGraph":
+        """The resident oriented CSR (nucleus34_ctx_copy_csr) as a HostGraph."""
+        n, m = self._nm
+        O = np.zeros(n + 1, np.uint32)
+        D = np.zeros(n, np.uint32)
+        E = np.zeros(m, np.uint32)
+        _check(self._L.nucleus34_ctx_copy_csr(self._h, _u32p(O), _u32p(D), _u32p(E)), "ctx_copy_csr")
+        return HostGraph(n, m, O, D, E)
 
     def run(self, variant="ondemand") -> dict:
         res = Result()

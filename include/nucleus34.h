@@ -170,6 +170,18 @@ int nucleus34_ctx_create(const nucleus34_opts *opts, nucleus34_ctx *out);
 /* H2D copy of the CSR into context-owned device memory (replaces the
  * thrust::device_vector uploads, cuNucleus34.cu:290-293). */
 int nucleus34_ctx_upload(nucleus34_ctx ctx, const nucleus34_csr *csr);
+/* The oriented CSR of an edge list, built on the device and made resident:
+ * the same graph as nucleus34_graph_from_edges followed by
+ * nucleus34_ctx_upload (symmetrise, drop self-loops, sort + unique,
+ * n = max id + 1 over the non-loop pairs, degree orientation; graph.hpp:
+ * 356-411, 176-218), with only the pairs crossing to the device. src and dst
+ * are host arrays of count pairs; *n_out and *m_out (optional) receive the
+ * vertex and oriented edge counts. */
+int nucleus34_ctx_upload_edges(nucleus34_ctx ctx, const uint32_t *src, const uint32_t *dst, uint64_t count,
+							   uint64_t *n_out, uint64_t *m_out);
+/* Copies the resident oriented CSR to the host: O (n+1 entries), D (n), E (m);
+ * each may be NULL. */
+int nucleus34_ctx_copy_csr(nucleus34_ctx ctx, uint32_t *O, uint32_t *D, uint32_t *E);
 /* Runs one decomposition of the resident graph; results stay on the device. */
 int nucleus34_ctx_run(nucleus34_ctx ctx, int variant, nucleus34_result *res);
 int nucleus34_ctx_copy_k(nucleus34_ctx ctx, int32_t *k_out, uint32_t *tris_out);

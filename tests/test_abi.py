@@ -57,6 +57,8 @@ def test_every_handle_entry_point_rejects_null_arguments(n34):
         "ctx_set_tune": lambda: L.nucleus34_ctx_set_tune(None, None),
         "ctx_last_tune": lambda: L.nucleus34_ctx_last_tune(None, None),
         "ctx_autotune": lambda: L.nucleus34_ctx_autotune(None, None, None, None, None),
+        "ctx_upload_edges": lambda: L.nucleus34_ctx_upload_edges(None, None, None, 0, None, None),
+        "ctx_copy_csr": lambda: L.nucleus34_ctx_copy_csr(None, None, None, None),
         "tune_lookup": lambda: L.nucleus34_tune_lookup(b"/tmp/unused", 0, 0, 0, 0, None, None),
         "tune_store": lambda: L.nucleus34_tune_store(b"/tmp/unused", 0, 0, 0, 0, None, 0.0, 0.0),
         "batch_decompose": lambda: L.nucleus34_batch_decompose(None, 1, None, None, None),
