@@ -164,12 +164,74 @@ __device__ __forceinline__ void gather_take(const Frontier fr, CtlX *ctl, bool t
 	}
 }
 
+// Level-change scans with 16-byte loads (build option N34_SCAN_VEC=1): each
+// thread reads eight consecutive supports per step, two aligned int4 loads,
+// so that a warp keeps 1 KB in flight instead of 128 bytes; a warp appends to
+// the frontier only in steps where one of its lanes takes a triangle.
+#ifndef N34_SCAN_VEC
+#define N34_SCAN_VEC 0
+#endif
+#if N34_SCAN_VEC
+constexpr uint32_t SCAN_VEC = 8;
+
+// v[j] = S[t0 + j] for t0 + j < T, else -1 (never taken); t0 is a multiple of
+// 8 and S is 256-byte aligned, so the vector loads are aligned.
+__device__ __forceinline__ void load_supports8(const int32_t *__restrict__ S, uint64_t T, uint64_t t0, int32_t v[8])
+{
+	if (t0 + SCAN_VEC <= T)
+	{
+		const int4 a = __ldg(reinterpret_cast<const int4 *>(S + t0));
+		const int4 b = __ldg(reinterpret_cast<const int4 *>(S + t0 + 4));
+		v[0] = a.x;
+		v[1] = a.y;
+		v[2] = a.z;
+		v[3] = a.w;
+		v[4] = b.x;
+		v[5] = b.y;
+		v[6] = b.z;
+		v[7] = b.w;
+	}
+	else
+	{
+#pragma unroll
+		for (uint32_t j = 0; j < SCAN_VEC; ++j)
+			v[j] = t0 + j < T ? S[t0 + j] : -1;
+	}
+}
+
+// Appends every t in [t0, t0 + 8) whose support is in [0, hi] (all lanes call).
+__device__ __forceinline__ void gather_range8(const Frontier fr, CtlX *ctl, const int32_t *__restrict__ S,
+											  uint64_t T, uint32_t hi)
+{
+	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x * SCAN_VEC;
+	for (uint64_t b0 = uint64_t(blockIdx.x) * blockDim.x * SCAN_VEC; b0 < T; b0 += stride)
+	{
+		const uint64_t t0 = b0 + uint64_t(threadIdx.x) * SCAN_VEC;
+		int32_t v[SCAN_VEC];
+		load_supports8(S, T, t0, v);
+		bool any = false;
+#pragma unroll
+		for (uint32_t j = 0; j < SCAN_VEC; ++j)
+			any = any || (v[j] >= 0 && uint32_t(v[j]) <= hi);
+		if (!__any_sync(FULL, any))
+			continue; // warp-uniform: b0 is the same for the whole block
+#pragma unroll
+		for (uint32_t j = 0; j < SCAN_VEC; ++j)
+			gather_take(fr, ctl, v[j] >= 0 && uint32_t(v[j]) <= hi, t0 + j, T);
+	}
+}
+#endif
+
 __global__ void __launch_bounds__(PEEL_THREADS) k_gather_next(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T,
 															  Frontier fr)
 {
 	if (ctl->c.done || !ctl->scan)
 		return;
 	const int32_t want = int32_t(ctl->c.level) + 1;
+#if N34_SCAN_VEC
+	gather_range8(fr, ctl, S, T, uint32_t(want));
+	return;
+#endif
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < T; t0 += stride)
 	{
@@ -196,6 +258,18 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int3
 	if (nf)
 		return;
 	uint32_t mn = INF;
+#if N34_SCAN_VEC
+	const uint64_t vstride = uint64_t(gridDim.x) * blockDim.x * SCAN_VEC;
+	for (uint64_t t0 = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * SCAN_VEC; t0 < T; t0 += vstride)
+	{
+		int32_t v[SCAN_VEC];
+		load_supports8(S, T, t0, v);
+#pragma unroll
+		for (uint32_t j = 0; j < SCAN_VEC; ++j)
+			if (v[j] >= 0)
+				mn = min(mn, uint32_t(v[j]));
+	}
+#else
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
 	{
@@ -203,6 +277,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int3
 		if (s >= 0)
 			mn = min(mn, uint32_t(s));
 	}
+#endif
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1)
 		mn = min(mn, __shfl_xor_sync(FULL, mn, o));
@@ -232,6 +307,10 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_
 	// every alive triangle sits above the old level, so the minimum is the new one
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		ctl->c.level = mn;
+#if N34_SCAN_VEC
+	gather_range8(fr, ctl, S, T, mn);
+	return;
+#endif
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < T; t0 += stride)
 	{
