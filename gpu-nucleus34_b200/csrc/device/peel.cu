@@ -38,6 +38,11 @@ namespace {
 
 constexpr uint32_t INF = 0xffffffffu;
 constexpr int PEEL_THREADS = 256;
+// Warp debit on one wave of blocks that claim frontier entries from an
+// atomic cursor (build option; off: a static warp stride over 2.7 waves).
+#ifndef N34_DEBIT_CURSOR
+#define N34_DEBIT_CURSOR 0
+#endif
 
 struct CtlX
 {
@@ -53,6 +58,9 @@ struct CtlX
 	// profiling counters of k_debit_flags_warp (filled only when stats is set)
 	uint32_t stats;
 	unsigned long long st_tri, st_merge_entries, st_steps, st_lookups, st_resolves, st_staged, st_found;
+#if N34_DEBIT_CURSOR
+	uint32_t cursor; // next unclaimed frontier position / bitmap word of the warp debit
+#endif
 };
 
 // A frontier is a list F[0, nF) (default) or, in the memory-lean peel, a
@@ -138,6 +146,9 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl, uint
 		ctl->compact_now = 0;
 		ctl->compact_div = compact_div;
 		ctl->sort_min = sort_min;
+#if N34_DEBIT_CURSOR
+		ctl->cursor = 0;
+#endif
 		ctl->peeled_at_compact = 0;
 		ctl->live_at_compact = T;
 		ctl->compactions = 0;
@@ -712,6 +723,26 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 #ifndef N34_DEBIT_MINB
 #define N34_DEBIT_MINB 6
 #endif
+#if N34_DEBIT_CURSOR
+// Claims the next `claim` positions below cap from *cursor into [cpos, cend);
+// false when none are left. Called by all lanes with warp-uniform values.
+// Positions are 32-bit: the death-flag peel has T <= 2^30, and the cursor
+// passes cap by at most one claim per warp.
+__device__ __forceinline__ bool claim_range(uint32_t *cursor, uint32_t claim, uint32_t cap, uint32_t &cpos,
+											uint32_t &cend)
+{
+	uint32_t b = 0;
+	if (lane_id() == 0)
+		b = atomicAdd(cursor, claim);
+	b = __shfl_sync(FULL, b, 0);
+	if (b >= cap)
+		return false;
+	cpos = b;
+	cend = cap - b > claim ? b + claim : cap;
+	return true;
+}
+#endif
+
 template <bool BITS, uint32_t LANE_MAX>
 __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
@@ -738,6 +769,42 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 	const uint32_t *F = ctl->c.cur ? F1 : F0;
 	const uint32_t *Bc = ctl->c.cur ? B1 : B0;
 	uint32_t word = 0; // bits of word fi not yet taken (bitmap mode)
+#if N34_DEBIT_CURSOR
+	// [cpos, cend): frontier positions (list) or bitmap words claimed by this
+	// warp; a claim takes CLAIM of them from the round's cursor (warp-uniform)
+	constexpr uint32_t CLAIM = BITS ? 4 : 16;
+	const uint32_t cap = BITS ? uint32_t(W) : nF;
+	uint32_t cpos = 0, cend = 0;
+	(void)warp;
+	(void)nwarps;
+	for (;;)
+	{
+		uint32_t t;
+		if (BITS)
+		{
+			// next nonzero word of the claim, claiming again when it is used up
+			while (!word)
+			{
+				if (cpos >= cend && !claim_range(&ctl->cursor, CLAIM, cap, cpos, cend))
+					break;
+				word = Bc[cpos];
+				if (!word)
+					++cpos;
+			}
+			if (!word)
+				break;
+			t = uint32_t(cpos * 32 + (__ffs(word) - 1));
+			word &= word - 1;
+			if (!word)
+				++cpos;
+		}
+		else
+		{
+			if (cpos >= cend && !claim_range(&ctl->cursor, CLAIM, cap, cpos, cend))
+				break;
+			t = F[cpos++];
+		}
+#else
 	// fi: list position, or bitmap word, advanced by the bitmap branch itself
 	for (uint64_t fi = warp;; fi += (BITS ? 0 : nwarps))
 	{
@@ -763,6 +830,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 				break;
 			t = F[fi];
 		}
+#endif
 		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 <= LANE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
@@ -1195,6 +1263,9 @@ __global__ void k_advance(CtlX *ctl)
 	c.nNext = 0;
 	c.minS = INF;
 	ctl->scan = c.nF == 0;
+#if N34_DEBIT_CURSOR
+	ctl->cursor = 0;
+#endif
 }
 
 __global__ void k_s_to_k(int32_t *__restrict__ S, uint64_t T)
@@ -1247,6 +1318,23 @@ void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool le
 	k_debit_flags_thread<LM><<<gscan, PEEL_THREADS, 0, st>>>(ctl, fr, tris, inc.span, inc.third, inc.tri, S, T);
 	if (ev5)
 		cudaEventRecord(ev5, st);
+#if N34_DEBIT_CURSOR
+	{
+		// one wave: as many blocks as can be resident at once on every SM
+		int dev = 0, sms = 1, per_sm = 1;
+		if (cudaGetDevice(&dev) != cudaSuccess ||
+			cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+			cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+				&per_sm, lean ? k_debit_flags_warp<true, LM> : k_debit_flags_warp<false, LM>, PEEL_THREADS, 0) !=
+				cudaSuccess ||
+			per_sm < 1)
+		{
+			cudaGetLastError();
+			per_sm = 1;
+		}
+		gwarp = uint32_t(per_sm) * uint32_t(sms > 0 ? sms : 1);
+	}
+#endif
 	if (lean)
 		k_debit_flags_warp<true, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
 																	 inc.span, inc.third, inc.tri, S, T);
