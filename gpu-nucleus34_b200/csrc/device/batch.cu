@@ -26,11 +26,16 @@
 
 // A batch is split into chunks whose unions stay within the 32-bit entry
 // positions of the incidence (3T < 2^32); each chunk is one device pass in
-// its own context, and its results stay resident until nucleus34_batch_free.
+// its own context, and its results stay resident until nucleus34_batch_free,
+// unless they were moved to host memory (hk, htris) to make room for a later
+// pass; the context then keeps only the per-graph statistics.
 struct BatchChunk
 {
 	nucleus34_ctx ctx = nullptr;
 	uint64_t first = 0, count = 0; // member graphs [first, first + count)
+	bool on_host = false;
+	std::vector<int32_t> hk;      // T (on_host)
+	std::vector<uint32_t> htris;  // 3T (on_host)
 };
 
 struct nucleus34_batch_s
@@ -310,6 +315,58 @@ void slice_union(const std::vector<uint32_t> &O, const std::vector<uint32_t> &D,
 
 using namespace n34;
 
+// Moves a finished pass's k and triangle list to host memory and frees its
+// device memory (results and graph); the per-graph statistics stay.
+static int move_results_to_host(BatchChunk &ch)
+{
+	Ctx &c = ch.ctx->c;
+	std::lock_guard<std::mutex> lk(c.mu);
+	if (ch.on_host)
+		return NUCLEUS34_OK;
+	N34_CUDA(cudaSetDevice(c.device));
+	const uint64_t T = c.T;
+	ch.hk.resize(T);
+	ch.htris.resize(3 * T);
+	if (T)
+	{
+		N34_CUDA(cudaMemcpyAsync(ch.hk.data(), c.dK, T * 4, cudaMemcpyDeviceToHost, c.stream));
+		N34_CUDA(cudaMemcpyAsync(ch.htris.data(), c.dtris, T * 12, cudaMemcpyDeviceToHost, c.stream));
+	}
+	N34_CUDA(cudaStreamSynchronize(c.stream));
+	std::vector<uint64_t> toff = std::move(c.seg_toff), q = std::move(c.seg_q), ks = std::move(c.seg_ksum);
+	std::vector<uint32_t> km = std::move(c.seg_kmax);
+	c.release_results();
+	c.release_graph();
+	c.seg_toff = std::move(toff);
+	c.seg_q = std::move(q);
+	c.seg_ksum = std::move(ks);
+	c.seg_kmax = std::move(km);
+	N34_CUDA(cudaStreamSynchronize(c.stream));
+	ch.on_host = true;
+	return NUCLEUS34_OK;
+}
+
+// Device memory a new context could use now: free memory plus what the
+// stream-ordered pool holds unused, at the 90% a default budget takes.
+static uint64_t device_room(int dev)
+{
+	size_t fb = 0, tb = 0;
+	if (cudaSetDevice(dev) != cudaSuccess || cudaMemGetInfo(&fb, &tb) != cudaSuccess)
+	{
+		cudaGetLastError();
+		return 0;
+	}
+	uint64_t cached = 0;
+	cudaMemPool_t pool;
+	uint64_t reserved = 0, used = 0;
+	if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess &&
+		cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+		cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used) == cudaSuccess && reserved > used)
+		cached = reserved - used;
+	cudaGetLastError();
+	return uint64_t(double(fb + cached) * 0.9);
+}
+
 template <class F>
 static int batch_guarded(F &&f)
 {
@@ -401,10 +458,25 @@ int nucleus34_batch_decompose(const nucleus34_csr *graphs, uint64_t count, const
 		cut.push_back(count);
 		const uint64_t nchunks = cut.size() - 1;
 		t_upload += std::chrono::duration<double>(std::chrono::steady_clock::now() - h0).count();
+		const bool to_host = opts && (opts->flags & NUCLEUS34_OPT_HOST_RESULTS);
+		const int dev = opts ? opts->device : 0;
 		for (uint64_t ci = 0; ci < nchunks; ++ci)
 		{
 			const uint64_t f = cut[ci], l = cut[ci + 1];
 			const auto c0 = std::chrono::steady_clock::now();
+			if (ci > 0 && !b->chunks.back().on_host)
+			{
+				// the results kept on the device must leave room for this pass
+				uint64_t tri = 0;
+				for (uint64_t g = f; g < l; ++g)
+					tri += tcount[g];
+				const uint64_t need = PASS_BYTES_PER_TRIANGLE * tri + 4 * (voff[l] - voff[f] + 1) +
+									  8 * (eoff[l] - eoff[f]);
+				if (to_host || need > device_room(dev))
+					for (auto &ch : b->chunks)
+						if ((rc = move_results_to_host(ch)))
+							return finish(rc);
+			}
 			nucleus34_ctx ctx = nullptr;
 			if (nchunks == 1)
 			{
@@ -452,6 +524,10 @@ int nucleus34_batch_decompose(const nucleus34_csr *graphs, uint64_t count, const
 			br.gpu_launches += r.gpu_launches;
 			br.peak_device_bytes = std::max<uint64_t>(br.peak_device_bytes, r.peak_device_bytes);
 		}
+		if (to_host)
+			for (auto &ch : b->chunks)
+				if ((rc = move_results_to_host(ch)))
+					return finish(rc);
 		br.t_upload = t_upload;
 		br.chunks = nchunks;
 		if (res)
@@ -503,6 +579,18 @@ int nucleus34_batch_copy_k(nucleus34_batch b, uint64_t index, int32_t *k_out, ui
 		const uint64_t t0 = c.seg_toff[i], T = c.seg_toff[i + 1] - t0;
 		if (!T)
 			return int(NUCLEUS34_OK);
+		if (ch->on_host)
+		{
+			if (k_out)
+				std::copy(ch->hk.begin() + t0, ch->hk.begin() + t0 + T, k_out);
+			if (tris_out)
+			{
+				const uint32_t eo = uint32_t(c.seg_eoff[i]);
+				for (uint64_t j = 0; j < 3 * T; ++j)
+					tris_out[j] = ch->htris[3 * t0 + j] - eo;
+			}
+			return int(NUCLEUS34_OK);
+		}
 		N34_CUDA(cudaSetDevice(c.device));
 		if (k_out)
 			N34_CUDA(cudaMemcpyAsync(k_out, c.dK + t0, T * 4, cudaMemcpyDeviceToHost, c.stream));

@@ -388,6 +388,7 @@ OPT_STAMP_PEEL = 0x1
 OPT_PROFILE_PEEL = 0x2
 OPT_LEAN_MEMORY = 0x4
 OPT_VERIFIABLE = 0x8
+OPT_HOST_RESULTS = 0x10
 
 
 def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1, flags: int = 0,

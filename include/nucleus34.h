@@ -93,6 +93,11 @@ typedef struct
 /* opts.flags: keep each triangle's death round after the peel, so that
  * nucleus34_ctx_verify can certify the result (costs 4 bytes per triangle). */
 #define NUCLEUS34_OPT_VERIFIABLE 0x8u
+/* opts.flags (batched form): each finished pass's k and triangle lists move
+ * to host memory and its device memory is freed before the next pass. Also
+ * chosen automatically when the next pass would not fit beside the results
+ * kept on the device. Results and accessors are unchanged. */
+#define NUCLEUS34_OPT_HOST_RESULTS 0x10u
 
 typedef struct
 {
