@@ -71,6 +71,9 @@ inline int run_program(const ProgramSpec &spec, int argc, char **argv)
 		j.raw(false, "data_loading_time_sec", fixed2(t_data));
 		if (spec.direct)
 			j.field(false, "data_memory_bytes", size_t(4 * (g.n + 1) + 4 * g.n + 4 * g.m));
+		mem_note("graph", "vertices=" + std::to_string(g.n) + " oriented_edges=" + std::to_string(g.m) +
+							  " host_graph=" + std::to_string((4 * (2 * g.n + 1) + 4 * g.m) >> 20) + " MiB load=" +
+							  secs1(t_data));
 
 		phase(step, spec.direct ? "1.1 Triangle counting, four-cliques and peeling (device)"
 								: "1.1 Triangle counting, incidence, support and peeling (device)");
@@ -86,6 +89,25 @@ inline int run_program(const ProgramSpec &spec, int argc, char **argv)
 		int rc = spec.direct ? nucleus34_decompose(&csr, &opts, &r, &h) : nucleus34_decompose_ondemand(&csr, &opts, &r, &h);
 		nucleus34_graph_release(&g);
 		check(rc, "decompose");
+		{
+			const uint64_t T = r.triangle_count, Q = r.four_clique_count;
+			if (spec.direct)
+			{
+				mem_note("tri-done", "triangles=" + std::to_string(T) + " device_tris=" +
+										 std::to_string((12 * T) >> 20) + " MiB time=" + secs1(r.t_triangles));
+				mem_note("fc-done", "four_cliques=" + std::to_string(Q) + " peak_device=" +
+										std::to_string(r.peak_device_bytes >> 20) + " MiB time=" + secs1(r.t_support));
+				if (Q)
+					mem_note("inc-done", "triangle->four-clique CSR built");
+			}
+			else
+			{
+				mem_note("incidence", "entries=" + std::to_string(r.incidence_entries) + " bytes=" +
+										  std::to_string((r.incidence_entries * 8) >> 20) + " MiB");
+				std::cerr << "[mem] support four_cliques=" << Q << " incidences=" << 4 * Q
+						  << " time=" << secs1(r.t_support) << std::endl;
+			}
+		}
 
 		const uint64_t T = r.triangle_count;
 		std::vector<int32_t> k(T);

@@ -281,6 +281,28 @@ inline void environment(Json &j, const char *app, const char *ver, bool direct, 
 	j.end();
 }
 
+// "[mem] <tag> <detail> | gpu_free=<free>/<total> MiB" on stderr: the
+// reference's memory milestone line (cuNucleus34.cu:72-79,
+// cuNucleus34_ondemand.cu:556-562, 585-588).
+inline void mem_note(const char *tag, const std::string &detail)
+{
+	size_t fb = 0, tb = 0;
+	if (cudaMemGetInfo(&fb, &tb) != cudaSuccess)
+	{
+		cudaGetLastError();
+		fb = tb = 0;
+	}
+	std::cerr << "[mem] " << tag << ' ' << detail << " | gpu_free=" << (fb >> 20) << "/" << (tb >> 20) << " MiB"
+			  << std::endl;
+}
+
+inline std::string secs1(double v)
+{
+	std::ostringstream os;
+	os << std::fixed << std::setprecision(1) << v << "s";
+	return os.str();
+}
+
 inline std::string fixed2(double v)
 {
 	std::ostringstream os;

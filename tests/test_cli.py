@@ -78,10 +78,12 @@ def test_handled_errors_go_into_the_record(prog, tmp_path, name, text, error):
 def test_record_holds_the_reader_counts(prog, tmp_path):
     path = tmp_path / "k4.edges"
     path.write_text(K4_TEXT)
-    rc, out, _ = run(prog, path)
+    rc, out, err = run(prog, path)
     assert rc == 0
     ds = record(out)["dataset"]
     assert ds["vertex_count"] == 5 and ds["edge_count"] == 12
+    # the reference's memory milestone line after the load (cuNucleus34.cu:272-279)
+    assert "[mem] graph vertices=5 oriented_edges=6 " in err and "| gpu_free=" in err
     if "error" in ds:  # no device here: the device step fails after the load
         assert ds["errorstep"].startswith("1.1 ")
     else:
