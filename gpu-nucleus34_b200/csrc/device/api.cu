@@ -9,7 +9,9 @@
 #include "pipeline.cuh"
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <exception>
 #include <new>
@@ -89,9 +91,28 @@ int set_device(Ctx &c)
 
 } // namespace
 
+// Failure injection for tests of the error paths: with
+// NUCLEUS34_FAIL_ALLOC_AT=N in the environment, the process's Nth device
+// allocation fails once with E_OOM_BUDGET (a host-side fake of an
+// out-of-memory; no device fault). Read once; unset means never.
+static bool injected_alloc_failure()
+{
+	static std::atomic<long long> countdown{[] {
+		const char *v = std::getenv("NUCLEUS34_FAIL_ALLOC_AT");
+		const long long n = v ? std::atoll(v) : 0;
+		return n > 0 ? n : 0LL;
+	}()};
+	if (countdown.load(std::memory_order_relaxed) <= 0)
+		return false;
+	return countdown.fetch_sub(1) == 1;
+}
+
 int Ctx::alloc(void **p, uint64_t bytes, const char *what)
 {
 	*p = nullptr;
+	if (injected_alloc_failure())
+		return fail(NUCLEUS34_E_OOM_BUDGET, std::string("injected allocation failure (NUCLEUS34_FAIL_ALLOC_AT) at ") +
+												what);
 	if (bytes == 0)
 		bytes = 16;
 	bytes = (bytes + 255) & ~uint64_t(255);
@@ -157,16 +178,11 @@ void Ctx::release_graph()
 	max_out = 0;
 }
 
-int upload(Ctx &c, const nucleus34_csr *csr)
+// The upload proper; upload() below releases the validation flag and, on any
+// failure, the partly uploaded graph, so that a failed upload leaves no graph
+// that a later run could take for a valid one.
+static int upload_graph(Ctx &c, const nucleus34_csr *csr, uint32_t *&bad)
 {
-	if (!csr || (csr->n && !csr->D) || (csr->m && !csr->E))
-		return fail(NUCLEUS34_E_INVALID, "null CSR array");
-	if (csr->m > 0xffffffffull || csr->n >= 0xffffffffull)
-		return fail(NUCLEUS34_E_RANGE32, "graph exceeds 32-bit vertex/edge ids");
-	N34_TRY(set_device(c));
-	c.release_results();
-	c.release_graph();
-	c.seg_eoff.clear();
 	const uint64_t n = csr->n, m = csr->m;
 	std::vector<uint32_t> O(n + 1);
 	uint64_t s = 0;
@@ -191,7 +207,6 @@ int upload(Ctx &c, const nucleus34_csr *csr)
 	c.n = n;
 	c.m = m;
 	c.max_out = max_out;
-	uint32_t *bad = nullptr;
 	N34_TRY(dalloc(c, &bad, 1, "validation flag"));
 	N34_CUDA(cudaMemsetAsync(bad, 0, 4, c.stream));
 	if (n)
@@ -199,16 +214,32 @@ int upload(Ctx &c, const nucleus34_csr *csr)
 	uint32_t hbad = 0;
 	N34_CUDA(cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, c.stream));
 	N34_CUDA(cudaStreamSynchronize(c.stream));
-	c.release(bad);
 	if (hbad)
-	{
-		c.release_graph();
-		return fail(NUCLEUS34_E_INVALID,
-					"CSR adjacency must hold ids < n, no self-loops, strictly ascending per vertex");
-	}
+		return fail(NUCLEUS34_E_INVALID, "CSR adjacency must hold ids < n, no self-loops, strictly ascending per vertex");
 	N34_TRY(build_src(c));
 	N34_CUDA(cudaStreamSynchronize(c.stream));
 	return NUCLEUS34_OK;
+}
+
+int upload(Ctx &c, const nucleus34_csr *csr)
+{
+	if (!csr || (csr->n && !csr->D) || (csr->m && !csr->E))
+		return fail(NUCLEUS34_E_INVALID, "null CSR array");
+	if (csr->m > 0xffffffffull || csr->n >= 0xffffffffull)
+		return fail(NUCLEUS34_E_RANGE32, "graph exceeds 32-bit vertex/edge ids");
+	N34_TRY(set_device(c));
+	c.release_results();
+	c.release_graph();
+	c.seg_eoff.clear();
+	uint32_t *bad = nullptr;
+	const int rc = upload_graph(c, csr, bad);
+	c.release(bad);
+	if (rc)
+	{
+		cudaStreamSynchronize(c.stream);
+		c.release_graph();
+	}
+	return rc;
 }
 
 // Settings of this run: the direct variant keeps the defaults (its clique
