@@ -218,8 +218,8 @@ int segments_after_peel(Ctx &c)
 }
 
 // Builds the union CSR of the member graphs on the host.
-int build_union(const nucleus34_csr *graphs, uint64_t count, std::vector<uint32_t> &O, std::vector<uint32_t> &D,
-				std::vector<uint32_t> &E, std::vector<uint64_t> &voff, std::vector<uint64_t> &eoff)
+int build_union(const nucleus34_csr *graphs, uint64_t count, HostU32 &O, HostU32 &D, HostU32 &E,
+				std::vector<uint64_t> &voff, std::vector<uint64_t> &eoff)
 {
 	voff.assign(count + 1, 0);
 	eoff.assign(count + 1, 0);
@@ -233,11 +233,16 @@ int build_union(const nucleus34_csr *graphs, uint64_t count, std::vector<uint32_
 	}
 	if (voff[count] >= 0xffffffffull || eoff[count] > 0xffffffffull)
 		return fail(NUCLEUS34_E_RANGE32, "batch union exceeds 32-bit vertex/edge ids");
-	O.assign(voff[count] + 1, 0);
-	D.assign(voff[count], 0);
-	E.assign(eoff[count], 0);
-	for (uint64_t g = 0; g < count; ++g)
+	O.resize(voff[count] + 1);
+	D.resize(voff[count]);
+	E.resize(eoff[count]);
+	// member graphs in parallel (disjoint ranges); a graph that fails its
+	// checks records why, and the first such graph is reported
+	std::vector<uint8_t> why(count, 0);
+#pragma omp parallel for schedule(dynamic, 8)
+	for (int64_t gi = 0; gi < int64_t(count); ++gi)
 	{
+		const uint64_t g = uint64_t(gi);
 		const nucleus34_csr &x = graphs[g];
 		uint64_t s = eoff[g];
 		for (uint64_t u = 0; u < x.n; ++u)
@@ -247,15 +252,25 @@ int build_union(const nucleus34_csr *graphs, uint64_t count, std::vector<uint32_
 			s += x.D[u];
 		}
 		if (s != eoff[g + 1])
-			return fail(NUCLEUS34_E_INVALID, "batch graph " + std::to_string(g) + ": sum of D does not equal m");
+		{
+			why[g] = 1;
+			continue;
+		}
 		const uint32_t vo = uint32_t(voff[g]);
 		for (uint64_t j = 0; j < x.m; ++j)
 		{
 			if (x.E[j] >= x.n)
-				return fail(NUCLEUS34_E_INVALID, "batch graph " + std::to_string(g) + ": edge id out of range");
+			{
+				why[g] = 2;
+				break;
+			}
 			E[eoff[g] + j] = x.E[j] + vo;
 		}
 	}
+	for (uint64_t g = 0; g < count; ++g)
+		if (why[g])
+			return fail(NUCLEUS34_E_INVALID, "batch graph " + std::to_string(g) +
+												 (why[g] == 1 ? ": sum of D does not equal m" : ": edge id out of range"));
 	O[voff[count]] = uint32_t(eoff[count]);
 	return NUCLEUS34_OK;
 }
@@ -297,18 +312,24 @@ int triangles_per_graph(Ctx &c, const std::vector<uint64_t> &voff, std::vector<u
 
 // Union of the member graphs [first, last) of the full union (O, D, E),
 // re-based to start at vertex 0 and edge 0.
-void slice_union(const std::vector<uint32_t> &O, const std::vector<uint32_t> &D, const std::vector<uint32_t> &E,
-				 const std::vector<uint64_t> &voff, const std::vector<uint64_t> &eoff, uint64_t first, uint64_t last,
-				 std::vector<uint32_t> &So, std::vector<uint32_t> &Sd, std::vector<uint32_t> &Se)
+void slice_union(const HostU32 &O, const HostU32 &D, const HostU32 &E, const std::vector<uint64_t> &voff,
+				 const std::vector<uint64_t> &eoff, uint64_t first, uint64_t last, HostU32 &So, HostU32 &Sd,
+				 HostU32 &Se)
 {
 	const uint64_t v0 = voff[first], v1 = voff[last], e0 = eoff[first], e1 = eoff[last];
 	So.resize(v1 - v0 + 1);
-	Sd.assign(D.begin() + v0, D.begin() + v1);
+	Sd.resize(v1 - v0);
 	Se.resize(e1 - e0);
-	for (uint64_t u = v0; u <= v1; ++u)
-		So[u - v0] = uint32_t(O[u] - e0);
-	for (uint64_t j = e0; j < e1; ++j)
-		Se[j - e0] = uint32_t(E[j] - v0);
+#pragma omp parallel for schedule(static)
+	for (int64_t u = int64_t(v0); u <= int64_t(v1); ++u)
+	{
+		So[uint64_t(u) - v0] = uint32_t(O[uint64_t(u)] - e0);
+		if (uint64_t(u) < v1)
+			Sd[uint64_t(u) - v0] = D[uint64_t(u)];
+	}
+#pragma omp parallel for schedule(static)
+	for (int64_t j = int64_t(e0); j < int64_t(e1); ++j)
+		Se[uint64_t(j) - e0] = uint32_t(E[uint64_t(j)] - v0);
 }
 
 } // namespace n34
@@ -395,7 +416,7 @@ int nucleus34_batch_decompose(const nucleus34_csr *graphs, uint64_t count, const
 	*out = nullptr;
 	return batch_guarded([&]() -> int {
 		const auto h0 = std::chrono::steady_clock::now();
-		std::vector<uint32_t> O, D, E;
+		HostU32 O, D, E;
 		std::vector<uint64_t> voff, eoff;
 		N34_TRY(build_union(graphs, count, O, D, E, voff, eoff));
 		auto *b = new (std::nothrow) nucleus34_batch_s();
@@ -492,7 +513,7 @@ int nucleus34_batch_decompose(const nucleus34_csr *graphs, uint64_t count, const
 				}
 				if ((rc = create_ctx(opts, &ctx)))
 					return finish(rc);
-				std::vector<uint32_t> So, Sd, Se;
+				HostU32 So, Sd, Se;
 				slice_union(O, D, E, voff, eoff, f, l, So, Sd, Se);
 				const nucleus34_csr u{voff[l] - voff[f], eoff[l] - eoff[f], So.data(), Sd.data(),
 									  Se.empty() ? nullptr : Se.data()};

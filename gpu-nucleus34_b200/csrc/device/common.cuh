@@ -6,9 +6,11 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <utility>
 #include <vector>
 
 #include "nucleus34.h"
@@ -139,6 +141,34 @@ struct Ctx
 	void release_results();
 	void release_graph();
 };
+
+// Host vectors whose resize leaves new elements uninitialised, for large
+// buffers that are written in full right after (batch unions and slices).
+template <class T>
+struct NoInitAlloc : std::allocator<T>
+{
+	template <class U>
+	struct rebind
+	{
+		using other = NoInitAlloc<U>;
+	};
+	NoInitAlloc() = default;
+	template <class U>
+	NoInitAlloc(const NoInitAlloc<U> &) noexcept
+	{
+	}
+	template <class U>
+	void construct(U *p) noexcept
+	{
+		::new (static_cast<void *>(p)) U;
+	}
+	template <class U, class... A>
+	void construct(U *p, A &&...a)
+	{
+		::new (static_cast<void *>(p)) U(std::forward<A>(a)...);
+	}
+};
+using HostU32 = std::vector<uint32_t, NoInitAlloc<uint32_t>>;
 
 template <class T>
 inline int dalloc(Ctx &c, T **p, uint64_t count, const char *what)

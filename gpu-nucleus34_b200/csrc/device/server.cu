@@ -27,8 +27,8 @@
 #include <vector>
 
 namespace n34 {
-int build_union(const nucleus34_csr *graphs, uint64_t count, std::vector<uint32_t> &O, std::vector<uint32_t> &D,
-				std::vector<uint32_t> &E, std::vector<uint64_t> &voff, std::vector<uint64_t> &eoff);
+int build_union(const nucleus34_csr *graphs, uint64_t count, HostU32 &O, HostU32 &D, HostU32 &E,
+				std::vector<uint64_t> &voff, std::vector<uint64_t> &eoff);
 }
 
 using namespace n34;
@@ -98,7 +98,7 @@ void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch)
 	for (size_t i = 0; i < batch.size(); ++i)
 		csrs[i] = nucleus34_csr{batch[i]->n, batch[i]->m, batch[i]->O.data(), batch[i]->D.data(),
 								batch[i]->E.empty() ? nullptr : batch[i]->E.data()};
-	std::vector<uint32_t> O, D, E;
+	HostU32 O, D, E;
 	std::vector<uint64_t> voff, eoff;
 	clear_error();
 	int rc = build_union(csrs.data(), csrs.size(), O, D, E, voff, eoff);
