@@ -79,6 +79,42 @@ def test_grh_round_trip(n34, tmp_path):
     assert np.array_equal(g.D, h.D) and np.array_equal(g.E, h.E) and np.array_equal(g.O, h.O)
 
 
+def test_grh_errors(n34, tmp_path):
+    """The .grh reader's failures (graph.hpp:491-520 layout: size_t sizeof(V),
+    nV, nE, then V D[nV], V E[nE]): another id width is the reference's
+    "Incompatible types in dataset."; a short file or a degree sum other
+    than nE is a format error; an empty graph loads."""
+    import struct
+    s, d = n34.gen_rmat(6, 8, 1)
+    g = n34.graph_from_edges(s, d)
+    p = str(tmp_path / "g.grh")
+    n34.save_grh(g, p)
+    raw = open(p, "rb").read()
+    assert struct.unpack("<QQQ", raw[:24]) == (4, g.n, g.m)
+
+    def load(data):
+        q = str(tmp_path / "x.grh")
+        open(q, "wb").write(data)
+        return n34.load_graph(q)
+
+    with pytest.raises(n34.Nucleus34Error) as e:
+        load(struct.pack("<Q", 8) + raw[8:])
+    assert e.value.code == n34.E_FORMAT and "Incompatible types" in str(e.value)
+    with pytest.raises(n34.Nucleus34Error) as e:
+        load(raw[:-4])
+    assert e.value.code == n34.E_FORMAT
+    with pytest.raises(n34.Nucleus34Error) as e:
+        load(raw[:12])
+    assert e.value.code == n34.E_FORMAT
+    D = np.frombuffer(raw[24:24 + 4 * g.n], np.uint32).copy()
+    D[0] += 1
+    with pytest.raises(n34.Nucleus34Error) as e:
+        load(raw[:24] + D.tobytes() + raw[24 + 4 * g.n:] + b"\0\0\0\0")
+    assert e.value.code == n34.E_FORMAT
+    empty = load(struct.pack("<QQQ", 4, 0, 0))
+    assert (empty.n, empty.m) == (0, 0)
+
+
 def test_library_and_oracle_build_the_same_csr(n34, oracle):
     for name, mk in graphs.SMALL.items():
         s, d = mk()
