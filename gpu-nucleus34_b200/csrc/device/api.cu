@@ -488,8 +488,10 @@ int autotune(Ctx &c, const char *path, nucleus34_tune *best_out, double *best_se
 		nucleus34_tune best = def;
 		double t_best = t_def;
 		const uint32_t NEVER = NUCLEUS34_TUNE_NEVER;
-		const std::vector<uint32_t> lanes = {8, 16, 32}, divs = {4, 8, 16, NEVER}, shifts = {10, 12, 14, NEVER},
-									rounds = {8, 16, 32};
+		// candidates around each default; replay length and compaction
+		// frequency move the peel the most, so they get the finest steps
+		const std::vector<uint32_t> lanes = {8, 16, 32}, divs = {4, 6, 8, 12, 16, NEVER},
+									shifts = {10, 11, 12, 13, 14, NEVER}, rounds = {8, 12, 16, 24, 32};
 		using Member = uint32_t nucleus34_tune::*;
 		struct Field
 		{
