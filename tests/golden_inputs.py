@@ -24,6 +24,7 @@ CASES = [
     {"name": "hubs3000_s2", "kind": "hubs", "n": 3000, "seed": 2, "ext": ".edges"},
     {"name": "cliques4to14", "kind": "cliques", "seed": 5, "ext": ".txt"},
     {"name": "k8_chain40_s6", "kind": "chain", "links": 40, "seed": 6, "ext": ".edges"},
+    {"name": "dense300_p05_s12", "kind": "dense", "n": 300, "p": 0.5, "seed": 12, "ext": ".edges"},
 ]
 
 QUIRKS_TXT = """# a comment line
@@ -91,7 +92,9 @@ def structured_pairs(case):
     cliques: disjoint K4..K14 joined by single bridge edges (k = n - 3 inside
       each clique);
     chain: K8s in a row, each sharing three vertices (a triangle) with the
-      next, plus a few random chords."""
+      next, plus a few random chords;
+    dense: G(n, p), every pair independently (long incidence lists on every
+      edge and a deep peel)."""
     rng = np.random.default_rng(case["seed"])
     kind = case["kind"]
     pairs = []
@@ -117,6 +120,11 @@ def structured_pairs(case):
                 pairs.append((prev, vs[int(rng.integers(0, size))]))
             prev = vs[-1]
             base += size
+    elif kind == "dense":
+        n = case["n"]
+        iu, ju = np.triu_indices(n, 1)
+        keep = rng.random(len(iu)) < case["p"]
+        pairs = list(zip(iu[keep].tolist(), ju[keep].tolist()))
     else:  # chain
         step = 5  # 8 vertices per clique, 3 shared with the next
         for c in range(case["links"]):
@@ -148,7 +156,7 @@ def materialise(case, directory):
             nucleus34.save_grh(nucleus34.graph_from_edges(s, d), path)
         else:
             nucleus34.write_edges(s, d, path)
-    elif kind in ("hubs", "cliques", "chain"):
+    elif kind in ("hubs", "cliques", "chain", "dense"):
         s, d = structured_pairs(case)
         nucleus34.write_edges(s, d, path)
     else:
