@@ -21,7 +21,6 @@
 // the caller.
 #include "pipeline.cuh"
 
-#include <mutex>
 #include <string>
 
 namespace n34 {
@@ -42,34 +41,52 @@ constexpr uint64_t NA_WORDS = NA_FLAG + 1;
 
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[NA_WORDS];
 
-std::mutex g_setup_mu;
-unsigned long long *g_scratch_ptr[64] = {}; // device address of the array, per ordinal
-
-// Per-device set-up: the address of the array as seen by device `dev` (the
-// device is current). Host code must not use the symbol's name as a pointer.
-int scratch_for(int dev, unsigned long long **out)
+// Set-up, run at the start of every call with the call's device current: the
+// address of the array as that device's current context sees it. Host code
+// must not use the symbol's name as a pointer (it names a host-side stand-in).
+// The address is not cached: a device reset reloads the module, and the array
+// may then sit elsewhere; the lookup costs far less than the call's own
+// synchronisation.
+int scratch_for_current_device(unsigned long long **out)
 {
-	if (dev < 0 || dev >= 64)
-		return fail(NUCLEUS34_E_INVALID, "device ordinal out of range");
-	std::lock_guard<std::mutex> lk(g_setup_mu);
-	if (!g_scratch_ptr[dev])
+	void *p = nullptr;
+	const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+	if (e != cudaSuccess || !p)
 	{
-		void *p = nullptr;
-		const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-		if (e != cudaSuccess || !p)
-		{
-			cudaGetLastError();
-			return fail(NUCLEUS34_E_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") +
-											  cudaGetErrorString(e));
-		}
-		g_scratch_ptr[dev] = static_cast<unsigned long long *>(p);
+		cudaGetLastError();
+		return fail(NUCLEUS34_E_CUDA, std::string("cudaGetSymbolAddress(no-alloc scratch): ") + cudaGetErrorString(e));
 	}
-	*out = g_scratch_ptr[dev];
+	*out = static_cast<unsigned long long *>(p);
 	return NUCLEUS34_OK;
 }
 
+// Makes `device` current for the call and gives the caller's current device
+// back on every return path.
+struct DeviceGuard
+{
+	int saved = -1;
+	cudaError_t enter(int device)
+	{
+		cudaError_t e = cudaGetDevice(&saved);
+		if (e != cudaSuccess)
+		{
+			saved = -1;
+			return e;
+		}
+		return saved == device ? cudaSuccess : cudaSetDevice(device);
+	}
+	~DeviceGuard()
+	{
+		int now = -1;
+		if (saved >= 0 && cudaGetDevice(&now) == cudaSuccess && now != saved)
+			cudaSetDevice(saved);
+	}
+};
+
 // Same checks as the context upload: ids < n, no self-loops, ascending lists,
-// O monotone with O[n] == m. Sets flag on any violation (the flag is cleared
+// O monotone with O[n] == m; and each undirected edge stored once: for an
+// edge u->v, u must not be in N+(v) (a symmetric CSR would list every
+// triangle more than once). Sets flag on any violation (the flag is cleared
 // by the host before this kernel).
 __global__ void k_na_validate(const uint32_t *__restrict__ O, const uint32_t *__restrict__ E, uint64_t n,
 							  uint64_t m, unsigned long long *__restrict__ flag)
@@ -87,8 +104,19 @@ __global__ void k_na_validate(const uint32_t *__restrict__ O, const uint32_t *__
 			const uint32_t v = E[j];
 			if (v >= n || v == u || (j > b && E[j - 1] >= v))
 				ok = false;
+			else
+			{
+				// reverse edge v->u present? (N+(v) is searched only within [O[v], O[v+1]) <= m)
+				const uint32_t vb = O[v], ve = O[v + 1];
+				if (vb <= ve && ve <= m)
+				{
+					const uint64_t pos = lower_bound_u32(E, vb, ve, uint32_t(u));
+					if (pos < ve && E[pos] == uint32_t(u))
+						ok = false;
+				}
+			}
 		}
-		if (!ok)
+		if (!__all_sync(FULL, ok) && lane_id() == 0)
 			atomicOr(flag, 1ull);
 	}
 }
@@ -208,11 +236,14 @@ int list_noalloc(const uint32_t *d_O, const uint32_t *d_E, uint64_t n, uint64_t 
 		return NUCLEUS34_OK;
 	if (!d_O || (m && !d_E) || (capacity && !d_tris))
 		return fail(NUCLEUS34_E_INVALID, "null device pointer");
-	N34_CUDA(cudaSetDevice(device));
+	DeviceGuard guard;
+	N34_CUDA(guard.enter(device));
 	unsigned long long *scr = nullptr;
-	N34_TRY(scratch_for(device, &scr));
-	cudaDeviceProp prop{};
-	N34_CUDA(cudaGetDeviceProperties(&prop, device));
+	N34_TRY(scratch_for_current_device(&scr));
+	int sms = 0;
+	N34_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+	if (sms < 1)
+		sms = 1;
 	cudaStream_t s = static_cast<cudaStream_t>(stream);
 	uint32_t *cnt = reinterpret_cast<uint32_t *>(scr + NA_COUNTS);
 	unsigned long long *off = scr + NA_OFFSETS;
@@ -225,7 +256,7 @@ int list_noalloc(const uint32_t *d_O, const uint32_t *d_E, uint64_t n, uint64_t 
 	N34_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned long long), s));
 	{
 		uint64_t g = (n + 7) / 8;
-		g = g > uint64_t(prop.multiProcessorCount) * 8 ? uint64_t(prop.multiProcessorCount) * 8 : g;
+		g = g > uint64_t(sms) * 8 ? uint64_t(sms) * 8 : g;
 		k_na_validate<<<uint32_t(g), 256, 0, s>>>(d_O, d_E, n, m, flag);
 		N34_CUDA(cudaGetLastError());
 	}
@@ -234,9 +265,10 @@ int list_noalloc(const uint32_t *d_O, const uint32_t *d_E, uint64_t n, uint64_t 
 	N34_CUDA(cudaStreamSynchronize(s));
 	if (hflag)
 		return fail(NUCLEUS34_E_INVALID,
-					"CSR must hold O[n] == m, ids < n, no self-loops, strictly ascending adjacency");
+					"CSR must hold O[n] == m, ids < n, no self-loops, strictly ascending adjacency and each "
+					"undirected edge once (no u->v beside v->u)");
 	// pass 1 counts (every entry of cnt[0..n) is written), scan, pass 2 writes
-	N34_CUDA(launch_tri_count(d_O, d_E, n, cnt, prop.multiProcessorCount, s));
+	N34_CUDA(launch_tri_count(d_O, d_E, n, cnt, sms, s));
 	k_na_tile_sums<<<tiles, 256, 0, s>>>(cnt, n, sums);
 	N34_CUDA(cudaGetLastError());
 	k_na_scan_sums<<<1, 1024, 0, s>>>(sums, tiles, bases);
@@ -252,8 +284,8 @@ int list_noalloc(const uint32_t *d_O, const uint32_t *d_E, uint64_t n, uint64_t 
 	if (T > capacity)
 		return fail(NUCLEUS34_E_INVALID, "output holds " + std::to_string(capacity) + " triangles, the graph has " +
 											 std::to_string(T) + " (the count is returned; call again with room)");
-	N34_CUDA(launch_tri_write(d_O, d_E, n, reinterpret_cast<const uint64_t *>(off), d_tris,
-							  prop.multiProcessorCount, s));
+	N34_CUDA(launch_tri_write(d_O, d_E, n, reinterpret_cast<const uint64_t *>(off), d_tris, sms,
+							  s));
 	N34_CUDA(cudaStreamSynchronize(s));
 	return NUCLEUS34_OK;
 }

@@ -363,16 +363,22 @@ void nucleus34_server_destroy(nucleus34_server s);
  * lists the triangles of an oriented CSR already in device memory, in
  * canonical (a,b) order, into a caller-owned device buffer, and allocates
  * nothing. d_O holds n+1 offsets (O[n] = m), d_E the m destinations; d_tris
- * receives 3 u32 per triangle. The count is always returned in
+ * receives 3 u32 per triangle. The CSR must be acyclically oriented with each
+ * undirected edge stored once and ascending adjacency lists, as
+ * nucleus34_graph_from_edges and nucleus34_graph_load produce; a CSR that
+ * breaks O[n] == m, holds an id >= n, a self-loop, an unsorted list or an
+ * edge stored in both directions is rejected with NUCLEUS34_E_INVALID and
+ * nothing is written (a longer cycle in the orientation is not detected: its
+ * triangles would be missed). The count is always returned in
  * *triangle_count; if it exceeds tris_capacity nothing is written and the
  * call returns NUCLEUS34_E_INVALID (call again with room; capacity 0 and a
  * NULL d_tris is a count-only query). At most 2^20 vertices: larger graphs
  * are rejected with NUCLEUS34_E_INVALID. The temporaries live in a fixed
  * static device array (about 12.6 MB, held by every GPU that loads the
  * library until exit) shared by all calls: calls that overlap on one GPU race
- * and must be serialised by the caller. The first call on a device resolves
- * that array's address on that device; make that first call before any stream
- * capture. stream is a cudaStream_t (NULL = default stream); the call
+ * and must be serialised by the caller. Every call looks up that array's
+ * address on `device` and restores the caller's current device before it
+ * returns. stream is a cudaStream_t (NULL = default stream); the call
  * synchronises it before returning. */
 int nucleus34_list_triangles_noalloc(const uint32_t *d_O, const uint32_t *d_E, uint64_t n, uint64_t m,
 									 uint32_t *d_tris, uint64_t tris_capacity, uint64_t *triangle_count,

@@ -91,7 +91,6 @@ def test_batch_cut_into_passes_by_memory_budget(n34):
 
 
 @pytest.mark.gpu
-@pytest.mark.skip(reason="batch results moved to host memory: first GPU run pending")
 def test_batch_results_moved_to_host_are_unchanged(n34):
     """NUCLEUS34_OPT_HOST_RESULTS moves every finished pass's k and triangle
     lists to host memory; summaries, k and triangle lists are those of the

@@ -6,6 +6,7 @@ import os
 import subprocess
 import sys
 
+import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -44,3 +45,37 @@ def test_reference_arm_runs_on_rank_zero_only():
                              "--cpu-sample-scale", 10, env={"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
     assert rc == 0, err
     assert out.strip() == ""
+
+
+def test_reference_arm_sample_generator_equals_the_library_generator(n34):
+    """The reference arm generates its sample in numpy (no library of this
+    project in that process); it must be the library's R-MAT edge for edge."""
+    sys.path.insert(0, ROOT)
+    import bench
+    for scale, ef, seed in ((6, 8, 1), (10, 16, 2), (12, 16, 5)):
+        s, d = n34.gen_rmat(scale, ef, seed)
+        bs, bd = bench.rmat_edges_numpy(scale, ef, seed)
+        assert np.array_equal(s, bs) and np.array_equal(d, bd), (scale, ef, seed)
+
+
+def test_reference_arm_sample_file_equals_the_library_writer(n34, tmp_path):
+    sys.path.insert(0, ROOT)
+    import bench
+    s, d = n34.gen_rmat(9, 8, 3)
+    n34.write_edges(s, d, str(tmp_path / "lib.edges"))
+    bench.write_edges_text(s, d, str(tmp_path / "np.edges"))
+    assert (tmp_path / "lib.edges").read_bytes() == (tmp_path / "np.edges").read_bytes()
+
+
+def test_reference_arm_loads_no_library_of_this_project():
+    """The reference arm's process maps none of this project's shared
+    libraries (only the reference's own program runs, as a child)."""
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '1', '--warmup', '0', "
+            "'--cpu-sample-scale', '9']\n"
+            "try:\n    runpy.run_path('bench.py', run_name='__main__')\nexcept SystemExit:\n    pass\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'libnucleus34' not in maps and 'liboracle' not in maps, 'a project library is mapped'\n"
+            "assert 'nucleus34' not in sys.modules\nprint('clean')\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().endswith("clean")

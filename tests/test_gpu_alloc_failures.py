@@ -12,10 +12,7 @@ import sys
 
 import pytest
 
-pytestmark = [
-    pytest.mark.gpu,
-    pytest.mark.skip(reason="allocation failure injection: first GPU run pending"),
-]
+pytestmark = pytest.mark.gpu
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 

@@ -7,10 +7,7 @@ an empty list and lists of self-loops only."""
 import numpy as np
 import pytest
 
-pytestmark = [
-    pytest.mark.gpu,
-    pytest.mark.skip(reason="device CSR build: first GPU run pending"),
-]
+pytestmark = pytest.mark.gpu
 
 
 def edge_cases(n34):

@@ -85,3 +85,46 @@ def test_noalloc_rejects_graphs_beyond_its_scratch(n34):
     assert rc == n34.E_INVALID
     assert "at most" in n34.last_error()
     assert cnt.value == 0
+
+
+def test_noalloc_rejects_malformed_csr_and_writes_nothing(n34):
+    """A CSR that breaks the input contract (O[n] != m, an unsorted list, an
+    edge stored in both directions, a self-loop) is refused before anything
+    is written, and the caller's current device is unchanged."""
+    import torch
+    s, d = n34.gen_rmat(9, 8, 3)
+    g = n34.graph_from_edges(s, d)
+    O = g.O[: g.n + 1].astype(np.uint32)
+    E = g.E.astype(np.uint32)
+    u = int(np.argmax(np.diff(O.astype(np.int64))))  # a vertex with at least two out-edges
+    assert O[u + 1] - O[u] >= 2
+    unsorted = E.copy()
+    unsorted[O[u]], unsorted[O[u] + 1] = unsorted[O[u] + 1], unsorted[O[u]]
+    loop = E.copy()
+    loop[O[u]] = u
+    # symmetric: every edge in both directions (a triangle would be listed several times)
+    src = np.repeat(np.arange(g.n, dtype=np.uint32), np.diff(O.astype(np.int64)))
+    both_s = np.concatenate([src, E])
+    both_d = np.concatenate([E, src])
+    order = np.lexsort((both_d, both_s))
+    both_s, both_d = both_s[order], both_d[order]
+    symO = np.zeros(g.n + 1, np.uint32)
+    np.add.at(symO, both_s.astype(np.int64) + 1, 1)
+    symO = np.cumsum(symO).astype(np.uint32)
+    bad_m = O.copy()
+    bad_m[-1] -= 1
+    cases = {"O[n] != m": (bad_m, E, g.m), "unsorted list": (O, unsorted, g.m), "self-loop": (O, loop, g.m),
+             "both directions": (symO, both_d, len(both_d))}
+    f = _entry(n34)
+    torch.cuda.set_device(0)
+    for name, (o, e, m) in cases.items():
+        dO = torch.from_numpy(o.view(np.int32).copy()).to("cuda:0")
+        dE = torch.from_numpy(e.view(np.int32).copy()).to("cuda:0")
+        out = torch.full((3 * 4096,), -1, dtype=torch.int32, device="cuda:0")
+        cnt = C.c_uint64(123)
+        rc = f(dO.data_ptr(), dE.data_ptr(), g.n, m, out.data_ptr(), 4096, C.byref(cnt), 0, None)
+        assert rc == n34.E_INVALID, name
+        assert "each undirected edge once" in n34.last_error(), name
+        assert cnt.value == 0, name
+        assert np.all(out.cpu().numpy() == -1), name
+        assert torch.cuda.current_device() == 0
