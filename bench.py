@@ -448,6 +448,12 @@ def capture_run(a):
     return 0
 
 
+def spread(xs):
+    """min / median / max of the timed steps, and (max - min) / median."""
+    med = statistics.median(xs)
+    return {"min": min(xs), "median": med, "max": max(xs), "spread": (max(xs) - min(xs)) / med if med else None}
+
+
 def max_over_ranks(x: float, device: str) -> float:
     """The slowest rank's time (all_reduce MAX over the process group): the
     job is done when its last replica is."""
@@ -611,6 +617,8 @@ def main():
                    "parallelism": f"replicas x{world} (one graph per GPU, no collective)",
                    "l2": "inputs > L2 and a 256 MiB L2-flush write between steps"},
         "phases_ms": {k: r[k] * 1e3 for k in ("t_triangles", "t_incidence", "t_support", "t_cliques", "t_peel")},
+        "steps_ms": {k: spread([x[k] * 1e3 for x in results])
+                     for k in ("t_total", "t_triangles", "t_incidence", "t_support", "t_peel")},
         "peel_rounds": int(r["peeling_iterations"]), "k_max": int(r["k_max"]),
         "peak_device_bytes": int(r["peak_device_bytes"]),
         "gpu_launches": int(launches),

@@ -66,6 +66,18 @@ constexpr uint32_t MERGE_RATIO = 24;
 #define N34_SAMPLE_MIN 256u
 #endif
 
+// Loads of the incidence's triangle words (which carry the death flags).
+// Kernels that only read them during their run use the read-only path; a
+// kernel that also writes flags in an earlier phase of the same launch (the
+// cooperative small-round peel) must read them through L2.
+template <bool COHERENT>
+__device__ __forceinline__ uint32_t ld_tri(const uint32_t *p)
+{
+	if (COHERENT)
+		return __ldcg(p);
+	return __ldg(p);
+}
+
 __device__ __forceinline__ bool use_merge(const Lists &L)
 {
 	return (L.b1 - L.b0) <= MERGE_RATIO * (L.a1 - L.a0);
@@ -166,7 +178,7 @@ __device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t *__restrict_
 // WITH_TRI also qa = itri[pa], qb = itri[pb] (the partner tiles are loaded
 // together with the third tiles, saving a dependent round trip). Each common
 // x is seen exactly once, in ascending order across steps.
-template <bool WITH_TRI, class F>
+template <bool WITH_TRI, class F, bool COH = false>
 __device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 											uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, F &&f)
 {
@@ -180,8 +192,8 @@ __device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, 
 		uint32_t at = 0, bt = 0;
 		if (WITH_TRI)
 		{
-			at = av_ok ? __ldg(itri + ai) : 0u;
-			bt = bv_ok ? __ldg(itri + bi) : 0u;
+			at = av_ok ? ld_tri<COH>(itri + ai) : 0u;
+			bt = bv_ok ? ld_tri<COH>(itri + bi) : 0u;
 		}
 		const uint32_t amax = __shfl_sync(FULL, av, 31), bmax = __shfl_sync(FULL, bv, 31);
 		const uint32_t m = amax < bmax ? amax : bmax;
@@ -205,7 +217,7 @@ __device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, 
 }
 
 // Warp binary search of A's entries in B (B much longer than A).
-template <bool WITH_TRI, class F>
+template <bool WITH_TRI, class F, bool COH = false>
 __device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 											 uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, F &&f)
 {
@@ -217,10 +229,10 @@ __device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third,
 		const uint32_t ai = base + lane;
 		const bool ok = ai < a1;
 		const uint32_t x = ok ? __ldg(third + ai) : 0xffffffffu;
-		const uint32_t at = (WITH_TRI && ok) ? __ldg(itri + ai) : 0u;
+		const uint32_t at = (WITH_TRI && ok) ? ld_tri<COH>(itri + ai) : 0u;
 		const uint32_t p = warp_lower_bound(third, b0, b1, ok, x);
 		const bool found = ok && p < b1 && __ldg(third + p) == x;
-		const uint32_t bt = (WITH_TRI && found) ? __ldg(itri + p) : 0u;
+		const uint32_t bt = (WITH_TRI && found) ? ld_tri<COH>(itri + p) : 0u;
 		f(found, x, ai, p, at, bt);
 		// later steps hold larger x: the highest searching lane's bound stays valid
 		const uint32_t msk = __ballot_sync(FULL, ok);
@@ -229,14 +241,14 @@ __device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third,
 }
 
 // Warp dispatch between merge and search for the two shortest lists.
-template <bool WITH_TRI = false, class F>
+template <bool WITH_TRI = false, bool COH = false, class F>
 __device__ __forceinline__ void warp_intersect2(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 												const Lists &L, F &&f)
 {
 	if (use_merge(L))
-		warp_merge2<WITH_TRI>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
+		warp_merge2<WITH_TRI, F &, COH>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
 	else
-		warp_search2<WITH_TRI>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
+		warp_search2<WITH_TRI, F &, COH>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
 }
 
 // One lane on its own: each entry of A binary-searched in B (the window only

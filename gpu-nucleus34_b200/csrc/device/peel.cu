@@ -38,6 +38,10 @@ namespace {
 
 constexpr uint32_t INF = 0xffffffffu;
 constexpr int PEEL_THREADS = 256;
+// The device loop stops a peel that has run this long (device time) and the
+// call returns NUCLEUS34_E_TIMEOUT: a bound on a loop that would otherwise
+// only end by the round bound. R-MAT scale 20 peels in about 2 s.
+constexpr unsigned long long PEEL_TIME_LIMIT_NS = 600ull * 1000000000ull;
 // Warp debit on one wave of blocks that claim frontier entries from an
 // atomic cursor (build option; off: a static warp stride over 2.7 waves).
 #ifndef N34_DEBIT_CURSOR
@@ -55,6 +59,8 @@ struct CtlX
 	unsigned long long peeled_at_compact;
 	unsigned long long live_at_compact;
 	uint32_t compactions;
+	unsigned long long t0_ns; // %globaltimer at the peel's start (device-loop time bound)
+	uint32_t timed_out;       // the device loop stopped at its round or time bound
 	// profiling counters of k_debit_flags_warp (filled only when stats is set)
 	uint32_t stats;
 	unsigned long long st_tri, st_merge_entries, st_steps, st_lookups, st_resolves, st_staged, st_found;
@@ -113,19 +119,6 @@ __device__ __forceinline__ void frontier_each_thread(const Frontier fr, uint32_t
 	}
 }
 
-// Adds triangle q to the next frontier (list append or bit), counting nNext.
-__device__ __forceinline__ void frontier_push(const Frontier fr, uint32_t cur, uint32_t q, uint32_t *nNext,
-											  uint64_t cap, uint32_t *err)
-{
-	const uint32_t slot = atomicAdd(nNext, 1u);
-	if (fr.bits())
-		atomicOr(fr.next_bits(cur) + (q >> 5), 1u << (q & 31));
-	else if (slot < cap)
-		fr.next_list(cur)[slot] = q;
-	else
-		atomicOr(err, 1u);
-}
-
 // K null: k is kept in S (a dead triangle holds -1 - k there), as in the
 // memory-lean peel; otherwise every k starts at -1 (not peeled).
 __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl, uint32_t compact_div,
@@ -151,6 +144,10 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl, uint
 #endif
 		ctl->peeled_at_compact = 0;
 		ctl->live_at_compact = T;
+		unsigned long long now;
+		asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+		ctl->t0_ns = now;
+		ctl->timed_out = 0;
 		ctl->compactions = 0;
 		ctl->st_tri = ctl->st_merge_entries = ctl->st_steps = ctl->st_lookups = 0;
 		ctl->st_resolves = ctl->st_staged = ctl->st_found = 0;
@@ -656,53 +653,6 @@ __device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q
 // shortest list are skipped before any search. After a compaction the entry
 // of a partner that died earlier is gone; a third that is not found on an edge
 // therefore means the clique was destroyed before.
-template <uint32_t LANE_MAX>
-__global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
-	CtlX *ctl, Frontier fr, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
-	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T)
-{
-	if (ctl->c.done)
-		return;
-	const uint32_t cur = ctl->c.cur;
-	const int32_t level = int32_t(ctl->c.level);
-	uint32_t *nNext = &ctl->c.nNext;
-	uint32_t *err = &ctl->c.error;
-	frontier_each_thread(fr, cur, ctl->c.nF, false, [&](uint32_t t) {
-		const Lists L = frontier_lists(t, tris, span);
-		if (L.a1 - L.a0 > LANE_MAX)
-			return; // the warp kernel takes it
-		uint32_t lo_b = L.b0, lo_c = L.c0;
-		for (uint32_t i = L.a0; i < L.a1 && lo_b < L.b1; ++i)
-		{
-			const uint32_t q0 = __ldg(itri + i);
-			if (q0 & DEAD)
-				continue;
-			const uint32_t x = __ldg(third + i);
-			lo_b = lower_bound32(third, lo_b, L.b1, x);
-			if (lo_b >= L.b1)
-				break;
-			if (__ldg(third + lo_b) != x)
-				continue;
-			const uint32_t q1 = __ldg(itri + lo_b);
-			if (q1 & DEAD)
-				continue;
-			lo_c = lower_bound32(third, lo_c, L.c1, x);
-			if (lo_c >= L.c1 || __ldg(third + lo_c) != x)
-				continue; // the partner on the longest list was compacted away
-			const uint32_t q2 = __ldg(itri + lo_c);
-			if (q2 & DEAD)
-				continue;
-			bool hit[3];
-			settle_flags(t, q0, q1, q2, S, level, hit);
-			const uint32_t qs[3] = {q0, q1, q2};
-#pragma unroll
-			for (int r = 0; r < 3; ++r)
-				if (hit[r])
-					frontier_push(fr, cur, qs[r], nNext, T, err);
-		}
-	});
-}
-
 // Debit of dying triangles with long lists: one warp each, tile merge (or
 // binary search) of the two shortest lists. A common third whose two
 // partners on A and B are alive is queued in shared memory; the queue is
@@ -743,6 +693,271 @@ __device__ __forceinline__ bool claim_range(uint32_t *cursor, uint32_t claim, ui
 }
 #endif
 
+// Shared memory of one warp of the warp debit: the queue of lookups on the
+// longest list, and a copy of that list's thirds when it is short.
+struct DebitSmem
+{
+	uint32_t *bx, *b0, *b1; // 64 entries each
+	uint32_t *cstage;       // N34_C_STAGE entries (unused when 0)
+};
+
+// Debit of one dying triangle t by one warp (all lanes call): tile merge (or
+// binary search) of the two shortest lists; a common third whose partners on
+// A and B are alive, and not owned by a dying partner of smaller id, is queued
+// in shared memory; the queue is resolved 32 entries at a time (each lane one
+// lookup on the longest list), so the dependent search chain is paid once per
+// 32 live cliques instead of once per merge step that has any. Next-frontier
+// appends go to the list Fn (or bitmap Bn with BITS). COH: the flags are read
+// through L2 (a kernel that wrote them earlier in the same launch).
+template <bool BITS, bool COH>
+__device__ __forceinline__ void debit_warp_tri(uint32_t t, const Lists &L, const DebitSmem &sm, CtlX *ctl,
+											   uint32_t *__restrict__ Fn, uint32_t *__restrict__ Bn,
+											   const uint32_t *__restrict__ third, const uint32_t *itri,
+											   int32_t *__restrict__ S, int32_t level, uint64_t T)
+{
+	const uint32_t lane = lane_id();
+	uint32_t *nNext = &ctl->c.nNext;
+	uint32_t *err = &ctl->c.error;
+	uint32_t *bx = sm.bx, *b0 = sm.b0, *b1 = sm.b1;
+#if N34_L2_PREFETCH
+	if (lane == 0 && use_merge(L))
+	{
+		prefetch_range_l2(third, L.a0, L.a1);
+		prefetch_range_l2(third, L.b0, L.b1);
+		prefetch_range_l2(itri, L.a0, L.a1);
+		prefetch_range_l2(itri, L.b0, L.b1);
+	}
+#endif
+#if N34_PEEL_STATS
+	const bool st = ctl->stats != 0;
+#else
+	constexpr bool st = false;
+#endif
+	unsigned long long n_steps = 0, n_lookups = 0, n_resolves = 0, n_staged = 0, n_found = 0;
+	uint32_t lo_c = L.c0;
+	uint32_t queued = 0; // warp-uniform
+	// How the lookups on C are served, decided at the first resolve
+	// (warp-uniform): 0 undecided, 1 from a copy of C's thirds staged in
+	// shared memory (C short against the lookups: one coalesced read of
+	// C instead of a search path per lookup), 2 by sampled binary
+	// searches in global memory (one sample of C per triangle).
+	uint32_t mode = 0, stage_base = 0, stage_len = 0;
+	WarpSample cs{0u, 0u, false};
+#if N34_C_STAGE > 0
+	uint32_t *cstage = sm.cstage;
+#endif
+	// resolves the first n (<= 32) queued entries; called by all lanes
+	auto resolve = [&](uint32_t n) {
+		__syncwarp();
+		if (mode == 0)
+		{
+			const uint32_t len = L.c1 - lo_c;
+#if N34_C_STAGE > 0
+			if (len <= N34_C_STAGE && len <= 32u * n)
+			{
+				for (uint32_t i = lane; i < len; i += 32)
+					cstage[i] = __ldg(third + lo_c + i);
+				__syncwarp();
+				stage_base = lo_c;
+				stage_len = len;
+				mode = 1;
+			}
+			else
+#endif
+			{
+				cs = warp_sample(third, lo_c, L.c1);
+				mode = 2;
+			}
+		}
+		const bool v = lane < n;
+		const uint32_t x = v ? bx[lane] : 0xffffffffu;
+		const uint32_t q0 = v ? b0[lane] : DEAD, q1 = v ? b1[lane] : DEAD;
+		uint32_t pc = L.c1, xc = 0xffffffffu, q2 = DEAD;
+#if N34_C_STAGE > 0
+		if (mode == 1)
+		{
+			if (v)
+			{
+				// lower bound of x in the staged thirds from lo_c on
+				uint32_t lo = lo_c - stage_base, cnt = stage_len - lo;
+				while (cnt > 0)
+				{
+					const uint32_t half = cnt >> 1;
+					const bool less = cstage[lo + half] < x;
+					lo = less ? lo + half + 1 : lo;
+					cnt = less ? cnt - half - 1 : half;
+				}
+				pc = stage_base + lo;
+				if (lo < stage_len)
+					xc = cstage[lo];
+				if (xc == x)
+					q2 = ld_tri<COH>(itri + pc);
+			}
+		}
+		else
+#endif
+		{
+			pc = sampled_lower_bound(third, cs, lo_c, L.c1, v, x);
+			if (v && pc < L.c1)
+			{
+				xc = __ldg(third + pc);
+				q2 = ld_tri<COH>(itri + pc);
+			}
+		}
+		lo_c = __shfl_sync(FULL, pc, n - 1); // thirds ascend through the queue
+		if (st)
+		{
+			n_lookups += n;
+			n_resolves += 1;
+			n_staged += mode == 1;
+			n_found += __popc(__ballot_sync(FULL, v && xc == x));
+		}
+		bool hit[3] = {false, false, false};
+		// absent from C: that partner died and was compacted away (clique destroyed)
+		if (v && xc == x && !(q2 & DEAD))
+			settle_flags(t, q0, q1, q2, S, level, hit);
+		const uint32_t qs[3] = {q0, q1, q2};
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+		{
+			const uint32_t slot = warp_append(hit[r], nNext);
+			if (hit[r])
+			{
+				if (BITS)
+					atomicOr(Bn + (qs[r] >> 5), 1u << (qs[r] & 31));
+				else if (slot < T)
+					Fn[slot] = qs[r];
+				else
+					atomicOr(err, 1u);
+			}
+		}
+		__syncwarp();
+	};
+	warp_intersect2<true, COH>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
+												   uint32_t qb) {
+		n_steps += st;
+		// a clique is looked up on C only if its partners on A and B are
+		// alive and neither is a dying triangle of smaller id (its owner)
+		const bool live = found && !(qa & DEAD) && !(qb & DEAD) && !((qa & DYING) && (qa & ID_MASK) < t) &&
+						  !((qb & DYING) && (qb & ID_MASK) < t);
+		const uint32_t fm = __ballot_sync(FULL, live);
+		if (!fm)
+			return;
+		const uint32_t o = queued + __popc(fm & lanemask_lt());
+		if (live)
+		{
+			bx[o] = x;
+			b0[o] = qa;
+			b1[o] = qb;
+		}
+		queued += __popc(fm);
+		if (queued >= 32)
+		{
+			resolve(32);
+			// move the overflow [32, queued) to the front (ranges do not overlap)
+			const uint32_t rest = queued - 32;
+			uint32_t mx = 0, m0 = 0, m1 = 0;
+			if (lane < rest)
+			{
+				mx = bx[32 + lane];
+				m0 = b0[32 + lane];
+				m1 = b1[32 + lane];
+			}
+			__syncwarp();
+			if (lane < rest)
+			{
+				bx[lane] = mx;
+				b0[lane] = m0;
+				b1[lane] = m1;
+			}
+			queued = rest;
+		}
+	});
+	if (queued)
+		resolve(queued);
+	__syncwarp();
+	if (st && lane == 0)
+	{
+		atomicAdd(&ctl->st_tri, 1ull);
+		atomicAdd(&ctl->st_merge_entries, (unsigned long long)(L.a1 - L.a0 + L.b1 - L.b0));
+		atomicAdd(&ctl->st_steps, n_steps);
+		atomicAdd(&ctl->st_lookups, n_lookups);
+		atomicAdd(&ctl->st_resolves, n_resolves);
+		atomicAdd(&ctl->st_staged, n_staged);
+		atomicAdd(&ctl->st_found, n_found);
+	}
+}
+
+// Debit of one dying triangle whose shortest list is short, by one thread
+// (see k_debit_flags_thread). Returns without work when the list is longer.
+template <uint32_t LANE_MAX, bool BITS, bool COH>
+__device__ __forceinline__ void debit_thread_tri(uint32_t t, const Lists &L, CtlX *ctl, uint32_t *__restrict__ Fn,
+												 uint32_t *__restrict__ Bn, const uint32_t *__restrict__ third,
+												 const uint32_t *itri, int32_t *__restrict__ S, int32_t level,
+												 uint64_t T)
+{
+	uint32_t lo_b = L.b0, lo_c = L.c0;
+	for (uint32_t i = L.a0; i < L.a1 && lo_b < L.b1; ++i)
+	{
+		const uint32_t q0 = ld_tri<COH>(itri + i);
+		if (q0 & DEAD)
+			continue;
+		const uint32_t x = __ldg(third + i);
+		lo_b = lower_bound32(third, lo_b, L.b1, x);
+		if (lo_b >= L.b1)
+			break;
+		if (__ldg(third + lo_b) != x)
+			continue;
+		const uint32_t q1 = ld_tri<COH>(itri + lo_b);
+		if (q1 & DEAD)
+			continue;
+		lo_c = lower_bound32(third, lo_c, L.c1, x);
+		if (lo_c >= L.c1 || __ldg(third + lo_c) != x)
+			continue; // the partner on the longest list was compacted away
+		const uint32_t q2 = ld_tri<COH>(itri + lo_c);
+		if (q2 & DEAD)
+			continue;
+		bool hit[3];
+		settle_flags(t, q0, q1, q2, S, level, hit);
+		const uint32_t qs[3] = {q0, q1, q2};
+#pragma unroll
+		for (int r = 0; r < 3; ++r)
+			if (hit[r])
+			{
+				const uint32_t slot = atomicAdd(&ctl->c.nNext, 1u);
+				if (BITS)
+					atomicOr(Bn + (qs[r] >> 5), 1u << (qs[r] & 31));
+				else if (slot < T)
+					Fn[slot] = qs[r];
+				else
+					atomicOr(&ctl->c.error, 1u);
+			}
+	}
+}
+
+template <uint32_t LANE_MAX>
+__global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
+	CtlX *ctl, Frontier fr, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
+	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T)
+{
+	if (ctl->c.done)
+		return;
+	const uint32_t cur = ctl->c.cur;
+	const int32_t level = int32_t(ctl->c.level);
+	uint32_t *Fn = fr.bits() ? nullptr : fr.next_list(cur);
+	uint32_t *Bn = fr.bits() ? fr.next_bits(cur) : nullptr;
+	const bool bits = fr.bits();
+	frontier_each_thread(fr, cur, ctl->c.nF, false, [&](uint32_t t) {
+		const Lists L = frontier_lists(t, tris, span);
+		if (L.a1 - L.a0 > LANE_MAX)
+			return; // the warp kernel takes it
+		if (bits)
+			debit_thread_tri<LANE_MAX, true, false>(t, L, ctl, Fn, Bn, third, itri, S, level, T);
+		else
+			debit_thread_tri<LANE_MAX, false, false>(t, L, ctl, Fn, Bn, third, itri, S, level, T);
+	});
+}
+
 template <bool BITS, uint32_t LANE_MAX>
 __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
@@ -759,10 +974,12 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 	uint32_t *Fn = ctl->c.cur ? F0 : F1;
 	uint32_t *Bn = ctl->c.cur ? B0 : B1;
 	const int32_t level = int32_t(ctl->c.level);
-	uint32_t *nNext = &ctl->c.nNext;
-	uint32_t *err = &ctl->c.error;
-	const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
-	uint32_t *bx = qx[wib], *b0 = qp0[wib], *b1 = qp1[wib];
+	const uint32_t wib = threadIdx.x >> 5;
+#if N34_C_STAGE > 0
+	const DebitSmem sm{qx[wib], qp0[wib], qp1[wib], cstage_all[wib]};
+#else
+	const DebitSmem sm{qx[wib], qp0[wib], qp1[wib], nullptr};
+#endif
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
 	const uint32_t nF = ctl->c.nF;
@@ -834,173 +1051,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 <= LANE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
-#if N34_L2_PREFETCH
-		if (lane == 0 && use_merge(L))
-		{
-			prefetch_range_l2(third, L.a0, L.a1);
-			prefetch_range_l2(third, L.b0, L.b1);
-			prefetch_range_l2(itri, L.a0, L.a1);
-			prefetch_range_l2(itri, L.b0, L.b1);
-		}
-#endif
-#if N34_PEEL_STATS
-		const bool st = ctl->stats != 0;
-#else
-		constexpr bool st = false;
-#endif
-		unsigned long long n_steps = 0, n_lookups = 0, n_resolves = 0, n_staged = 0, n_found = 0;
-		uint32_t lo_c = L.c0;
-		uint32_t queued = 0; // warp-uniform
-		// How the lookups on C are served, decided at the first resolve
-		// (warp-uniform): 0 undecided, 1 from a copy of C's thirds staged in
-		// shared memory (C short against the lookups: one coalesced read of
-		// C instead of a search path per lookup), 2 by sampled binary
-		// searches in global memory (one sample of C per triangle).
-		uint32_t mode = 0, stage_base = 0, stage_len = 0;
-		WarpSample cs{0u, 0u, false};
-#if N34_C_STAGE > 0
-		uint32_t *cstage = cstage_all[wib];
-#endif
-		// resolves the first n (<= 32) queued entries; called by all lanes
-		auto resolve = [&](uint32_t n) {
-			__syncwarp();
-			if (mode == 0)
-			{
-				const uint32_t len = L.c1 - lo_c;
-#if N34_C_STAGE > 0
-				if (len <= N34_C_STAGE && len <= 32u * n)
-				{
-					for (uint32_t i = lane; i < len; i += 32)
-						cstage[i] = __ldg(third + lo_c + i);
-					__syncwarp();
-					stage_base = lo_c;
-					stage_len = len;
-					mode = 1;
-				}
-				else
-#endif
-				{
-					cs = warp_sample(third, lo_c, L.c1);
-					mode = 2;
-				}
-			}
-			const bool v = lane < n;
-			const uint32_t x = v ? bx[lane] : 0xffffffffu;
-			const uint32_t q0 = v ? b0[lane] : DEAD, q1 = v ? b1[lane] : DEAD;
-			uint32_t pc = L.c1, xc = 0xffffffffu, q2 = DEAD;
-#if N34_C_STAGE > 0
-			if (mode == 1)
-			{
-				if (v)
-				{
-					// lower bound of x in the staged thirds from lo_c on
-					uint32_t lo = lo_c - stage_base, cnt = stage_len - lo;
-					while (cnt > 0)
-					{
-						const uint32_t half = cnt >> 1;
-						const bool less = cstage[lo + half] < x;
-						lo = less ? lo + half + 1 : lo;
-						cnt = less ? cnt - half - 1 : half;
-					}
-					pc = stage_base + lo;
-					if (lo < stage_len)
-						xc = cstage[lo];
-					if (xc == x)
-						q2 = __ldg(itri + pc);
-				}
-			}
-			else
-#endif
-			{
-				pc = sampled_lower_bound(third, cs, lo_c, L.c1, v, x);
-				if (v && pc < L.c1)
-				{
-					xc = __ldg(third + pc);
-					q2 = __ldg(itri + pc);
-				}
-			}
-			lo_c = __shfl_sync(FULL, pc, n - 1); // thirds ascend through the queue
-			if (st)
-			{
-				n_lookups += n;
-				n_resolves += 1;
-				n_staged += mode == 1;
-				n_found += __popc(__ballot_sync(FULL, v && xc == x));
-			}
-			bool hit[3] = {false, false, false};
-			// absent from C: that partner died and was compacted away (clique destroyed)
-			if (v && xc == x && !(q2 & DEAD))
-				settle_flags(t, q0, q1, q2, S, level, hit);
-			const uint32_t qs[3] = {q0, q1, q2};
-#pragma unroll
-			for (int r = 0; r < 3; ++r)
-			{
-				const uint32_t slot = warp_append(hit[r], nNext);
-				if (hit[r])
-				{
-					if (BITS)
-						atomicOr(Bn + (qs[r] >> 5), 1u << (qs[r] & 31));
-					else if (slot < T)
-						Fn[slot] = qs[r];
-					else
-						atomicOr(err, 1u);
-				}
-			}
-			__syncwarp();
-		};
-		warp_intersect2<true>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
-												  uint32_t qb) {
-			n_steps += st;
-			// a clique is looked up on C only if its partners on A and B are
-			// alive and neither is a dying triangle of smaller id (its owner)
-			const bool live = found && !(qa & DEAD) && !(qb & DEAD) &&
-							  !((qa & DYING) && (qa & ID_MASK) < t) && !((qb & DYING) && (qb & ID_MASK) < t);
-			const uint32_t fm = __ballot_sync(FULL, live);
-			if (!fm)
-				return;
-			const uint32_t o = queued + __popc(fm & lanemask_lt());
-			if (live)
-			{
-				bx[o] = x;
-				b0[o] = qa;
-				b1[o] = qb;
-			}
-			queued += __popc(fm);
-			if (queued >= 32)
-			{
-				resolve(32);
-				// move the overflow [32, queued) to the front (ranges do not overlap)
-				const uint32_t rest = queued - 32;
-				uint32_t mx = 0, m0 = 0, m1 = 0;
-				if (lane < rest)
-				{
-					mx = bx[32 + lane];
-					m0 = b0[32 + lane];
-					m1 = b1[32 + lane];
-				}
-				__syncwarp();
-				if (lane < rest)
-				{
-					bx[lane] = mx;
-					b0[lane] = m0;
-					b1[lane] = m1;
-				}
-				queued = rest;
-			}
-		});
-		if (queued)
-			resolve(queued);
-		__syncwarp();
-		if (st && lane == 0)
-		{
-			atomicAdd(&ctl->st_tri, 1ull);
-			atomicAdd(&ctl->st_merge_entries, (unsigned long long)(L.a1 - L.a0 + L.b1 - L.b0));
-			atomicAdd(&ctl->st_steps, n_steps);
-			atomicAdd(&ctl->st_lookups, n_lookups);
-			atomicAdd(&ctl->st_resolves, n_resolves);
-			atomicAdd(&ctl->st_staged, n_staged);
-			atomicAdd(&ctl->st_found, n_found);
-		}
+		debit_warp_tri<BITS, false>(t, L, sm, ctl, Fn, Bn, third, itri, S, level, T);
 	}
 }
 
@@ -1268,6 +1319,244 @@ __global__ void k_advance(CtlX *ctl)
 #endif
 }
 
+// ---- small rounds in one cooperative launch ----------------------------------
+//
+// Most rounds of a peel are small cascades (R-MAT scale 20: about 4300 of 5500
+// rounds have fewer than 2^16 dying triangles), and as separate launches each
+// pays a dozen kernels' fixed cost. k_small_rounds runs such rounds back to
+// back in one cooperative launch: mark, debit, finalize and advance of a round
+// are phases separated by grid barriers. It returns as soon as the frontier
+// is empty (a level change: the regular kernels scan), larger than
+// small_max, or the peel is done; the regular round that follows takes over.
+// The rules are those of the regular kernels (same device functions); flags
+// written in one phase are read in the next through L2 (__ldcg), never
+// through the read-only path.
+
+struct GridBar
+{
+	unsigned int count; // blocks arrived at the current barrier
+	unsigned int gen;   // barriers completed
+	unsigned int abort; // a wait ran past its time bound
+	unsigned int pad;
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+	unsigned long long t;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+	return t;
+}
+
+// Barrier of all blocks of a cooperative launch (all resident at once by
+// construction). Waits are bounded: past the deadline a block sets abort and
+// leaves; every block then sees abort (here or at its next barrier) and
+// returns false, so the kernel ends in any case.
+__device__ __forceinline__ bool grid_barrier(GridBar *bar, uint32_t &gen, unsigned long long deadline)
+{
+	__shared__ uint32_t ok_s;
+	__syncthreads();
+	if (threadIdx.x == 0)
+	{
+		__threadfence();
+		const uint32_t g = gen;
+		if (atomicAdd(&bar->count, 1u) == gridDim.x - 1)
+		{
+			atomicExch(&bar->count, 0u);
+			__threadfence();
+			atomicExch(&bar->gen, g + 1);
+		}
+		else
+		{
+			uint32_t spins = 0;
+			while (__ldcg(&bar->gen) == g)
+			{
+				if (__ldcg(&bar->abort))
+					break;
+				if ((++spins & 255u) == 0 && global_ns() > deadline)
+				{
+					atomicExch(&bar->abort, 1u);
+					break;
+				}
+				__nanosleep(64);
+			}
+		}
+		gen = g + 1;
+		__threadfence();
+		ok_s = __ldcg(&bar->abort) == 0;
+	}
+	__syncthreads();
+	return ok_s != 0;
+}
+
+#ifndef N34_SMALL_MAX
+#define N34_SMALL_MAX 8192u
+#endif
+// Time bound of one k_small_rounds launch (its rounds take microseconds each).
+constexpr unsigned long long SMALL_ROUNDS_LIMIT_NS = 10ull * 1000000000ull;
+// Rounds of one k_small_rounds launch at most (each peels at least one triangle).
+constexpr uint32_t SMALL_ROUNDS_MAX_ITER = 1u << 16;
+
+template <uint32_t LANE_MAX>
+__global__ void __launch_bounds__(PEEL_THREADS, 4) k_small_rounds(
+	CtlX *ctl, GridBar *bar, uint32_t *F0, uint32_t *F1, const uint32_t *__restrict__ tris,
+	const uint32_t *__restrict__ src, const uint32_t *__restrict__ E, const uint2 *__restrict__ span,
+	const uint32_t *__restrict__ third, const uint32_t *__restrict__ tpos, uint32_t *itri, uint64_t n3,
+	int32_t *K, int32_t *S, uint32_t *R, uint64_t T, uint32_t small_max)
+{
+	constexpr int WARPS = PEEL_THREADS / 32;
+	__shared__ uint32_t qx[WARPS][64], qp0[WARPS][64], qp1[WARPS][64];
+#if N34_C_STAGE > 0
+	__shared__ uint32_t cstage_all[WARPS][N34_C_STAGE];
+#endif
+	__shared__ uint32_t s_go, s_nF, s_cur, s_level, s_round;
+	const uint32_t lane = lane_id(), wib = threadIdx.x >> 5;
+#if N34_C_STAGE > 0
+	const DebitSmem sm{qx[wib], qp0[wib], qp1[wib], cstage_all[wib]};
+#else
+	const DebitSmem sm{qx[wib], qp0[wib], qp1[wib], nullptr};
+#endif
+	const uint64_t tid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+	const uint64_t nthreads = uint64_t(gridDim.x) * blockDim.x;
+	const uint64_t warp = tid >> 5, nwarps = nthreads >> 5;
+	uint32_t gen = 0;
+	if (threadIdx.x == 0)
+		gen = __ldcg(&bar->gen);
+	const unsigned long long deadline = global_ns() + SMALL_ROUNDS_LIMIT_NS;
+	bool aborted = false;
+	for (uint32_t it = 0; it < SMALL_ROUNDS_MAX_ITER; ++it)
+	{
+		if (threadIdx.x == 0)
+		{
+			const uint32_t nF = __ldcg(&ctl->c.nF);
+			s_go = !__ldcg(&ctl->c.done) && !__ldcg(&ctl->c.error) && !__ldcg(&ctl->scan) && nF > 0 &&
+				   nF <= small_max;
+			s_nF = nF;
+			s_cur = __ldcg(&ctl->c.cur);
+			s_level = __ldcg(&ctl->c.level);
+			s_round = __ldcg(&ctl->c.round);
+		}
+		__syncthreads();
+		if (!s_go) // the same for every block: ctl was last written before a barrier
+			break;
+		const uint32_t nF = s_nF, cur = s_cur, round = s_round;
+		const int32_t level = int32_t(s_level);
+		const uint32_t *F = cur ? F1 : F0;
+		uint32_t *Fn = cur ? F0 : F1;
+		// mark: k and the dying flag of every frontier triangle
+		for (uint64_t i = tid; i < nF; i += nthreads)
+		{
+			const uint32_t t = __ldcg(F + i);
+			if (K)
+				K[t] = level;
+			S[t] = -1 - level;
+			if (R)
+				R[t] = round;
+			uint64_t pos[3];
+			entry_positions(t, tris, src, E, span, third, tpos, pos);
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+				if (pos[r] < n3)
+					itri[pos[r]] = t | DYING;
+		}
+		if (!grid_barrier(bar, gen, deadline))
+		{
+			aborted = true;
+			break;
+		}
+		// debit: a warp takes 32 frontier entries; short ones a lane each,
+		// then the long ones one after the other with the whole warp
+		for (uint64_t base = warp * 32; base < nF; base += nwarps * 32)
+		{
+			const uint64_t i = base + lane;
+			const bool have = i < nF;
+			uint32_t t = 0;
+			Lists L{0, 0, 0, 0, 0, 0};
+			if (have)
+			{
+				t = __ldcg(F + i);
+				L = frontier_lists(t, tris, span);
+			}
+			const bool is_long = have && (L.a1 - L.a0 > LANE_MAX);
+			if (have && !is_long)
+				debit_thread_tri<LANE_MAX, false, true>(t, L, ctl, Fn, nullptr, third, itri, S, level, T);
+			uint32_t longs = __ballot_sync(FULL, is_long);
+			while (longs)
+			{
+				const uint32_t sl = __ffs(longs) - 1;
+				longs &= longs - 1;
+				const uint32_t tt = __shfl_sync(FULL, t, sl);
+				const Lists LL{__shfl_sync(FULL, L.a0, sl), __shfl_sync(FULL, L.a1, sl), __shfl_sync(FULL, L.b0, sl),
+							   __shfl_sync(FULL, L.b1, sl), __shfl_sync(FULL, L.c0, sl), __shfl_sync(FULL, L.c1, sl)};
+				debit_warp_tri<false, true>(tt, LL, sm, ctl, Fn, nullptr, third, itri, S, level, T);
+			}
+		}
+		if (!grid_barrier(bar, gen, deadline))
+		{
+			aborted = true;
+			break;
+		}
+		// finalize: dying -> dead
+		for (uint64_t i = tid; i < nF; i += nthreads)
+		{
+			const uint32_t t = __ldcg(F + i);
+			uint64_t pos[3];
+			entry_positions(t, tris, src, E, span, third, tpos, pos);
+#pragma unroll
+			for (int r = 0; r < 3; ++r)
+				if (pos[r] < n3)
+					itri[pos[r]] = t | DEAD;
+		}
+		if (!grid_barrier(bar, gen, deadline))
+		{
+			aborted = true;
+			break;
+		}
+		// advance (as k_advance)
+		if (blockIdx.x == 0 && threadIdx.x == 0)
+		{
+			PeelCtl &c = ctl->c;
+			const uint32_t nNext = __ldcg(&c.nNext);
+			c.peeled += nF;
+			c.rounds++;
+			c.round = round + 1;
+			c.cur = cur ^ 1u;
+			c.nF = nNext;
+			c.nNext = 0;
+			c.minS = INF;
+			ctl->scan = nNext == 0;
+#if N34_DEBIT_CURSOR
+			ctl->cursor = 0;
+#endif
+		}
+		if (!grid_barrier(bar, gen, deadline))
+		{
+			aborted = true;
+			break;
+		}
+	}
+	if (aborted && threadIdx.x == 0)
+	{
+		atomicOr(&ctl->c.error, 4u);
+		atomicExch(&ctl->timed_out, 1u);
+	}
+}
+
+// End of one pass of the device loop's body: go on while the peel is neither
+// done nor failed, within its round bound and its time bound.
+__global__ void k_loop_cond(CtlX *ctl, cudaGraphConditionalHandle h, uint32_t max_rounds,
+							unsigned long long limit_ns)
+{
+	unsigned long long now;
+	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+	bool more = !ctl->c.done && !ctl->c.error;
+	if (more && (ctl->c.round > max_rounds || now - ctl->t0_ns > limit_ns))
+	{
+		ctl->timed_out = 1;
+		more = false;
+	}
+	cudaGraphSetConditional(h, more ? 1u : 0u);
+}
+
 __global__ void k_s_to_k(int32_t *__restrict__ S, uint64_t T)
 {
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
@@ -1343,6 +1632,40 @@ void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool le
 																	  inc.span, inc.third, inc.tri, S, T);
 }
 
+// Cooperative launch of k_small_rounds (capturable into a CUDA graph).
+template <uint32_t LM>
+cudaError_t launch_small_rounds(cudaStream_t st, uint32_t grid, CtlX *ctl, GridBar *bar, const Frontier &fr,
+								const uint32_t *tris, const uint32_t *src, const uint32_t *E, const Incidence &inc,
+								int32_t *K, int32_t *S, uint32_t *R, uint64_t T, uint32_t small_max)
+{
+	cudaLaunchConfig_t cfg{};
+	cfg.gridDim = dim3(grid);
+	cfg.blockDim = dim3(PEEL_THREADS);
+	cfg.dynamicSmemBytes = 0;
+	cfg.stream = st;
+	cudaLaunchAttribute at[1];
+	at[0].id = cudaLaunchAttributeCooperative;
+	at[0].val.cooperative = 1;
+	cfg.attrs = at;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, k_small_rounds<LM>, ctl, bar, fr.F0, fr.F1, tris, src, E,
+							  static_cast<const uint2 *>(inc.span), static_cast<const uint32_t *>(inc.third),
+							  static_cast<const uint32_t *>(inc.tpos), inc.tri, uint64_t(3 * T), K, S, R, T, small_max);
+}
+
+template <uint32_t LM>
+uint32_t small_rounds_grid(int sm_count)
+{
+	int per_sm = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_small_rounds<LM>, PEEL_THREADS, 0) != cudaSuccess ||
+		per_sm < 1)
+	{
+		cudaGetLastError();
+		return 0;
+	}
+	return uint32_t(per_sm) * uint32_t(sm_count);
+}
+
 } // namespace
 
 int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_t *S, int32_t *K, PeelCtl *hctl)
@@ -1352,6 +1675,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			 *fchunk = nullptr;
 	uint8_t *destroyed = nullptr;
 	CtlX *ctl = nullptr;
+	GridBar *bar = nullptr;
 	int rc = NUCLEUS34_OK;
 	auto cleanup = [&] {
 		c.release(R);
@@ -1362,6 +1686,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		c.release(fbits);
 		c.release(fchunk);
 		c.release(ctl);
+		c.release(bar);
 		c.release(destroyed);
 	};
 	// death flags live in the incidence entries when triangle ids leave the
@@ -1414,6 +1739,34 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		const Frontier fr{F0, F1, B0, B1, fwords};
 		if ((rc = dalloc(c, &ctl, 1, "peel control")))
 			break;
+		// Small cascade rounds in one cooperative launch (death-flag peel with
+		// list frontiers; not in profiling mode, whose per-step events need the
+		// separate kernels).
+		const bool profile_mode = (c.opt_flags & NUCLEUS34_OPT_PROFILE_PEEL) != 0;
+		uint32_t gsmall = 0;
+		if (flags && !lean && !profile_mode && !(c.opt_flags & NUCLEUS34_OPT_NO_SMALL_ROUNDS))
+		{
+			int coop = 0;
+			if (cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c.device) != cudaSuccess)
+				coop = 0;
+			cudaGetLastError();
+			if (coop)
+				gsmall = tn.lane_max == 8	 ? small_rounds_grid<8>(c.sm_count)
+						 : tn.lane_max == 32 ? small_rounds_grid<32>(c.sm_count)
+											 : small_rounds_grid<THREAD_MODE_MAX>(c.sm_count);
+		}
+		if (gsmall)
+		{
+			if ((rc = dalloc(c, &bar, 1, "peel grid barrier")))
+				break;
+			if (cudaMemsetAsync(bar, 0, sizeof(GridBar), c.stream) != cudaSuccess)
+			{
+				rc = fail(NUCLEUS34_E_CUDA, "memset");
+				break;
+			}
+		}
+		const uint32_t small_max =
+			uint32_t(std::min<unsigned long long>(N34_SMALL_MAX, sort_min > 0 ? sort_min - 1 : 0));
 		// frontier ordering bitmap (optional: skipped without room for it;
 		// a bitmap frontier is in id order already)
 		const uint64_t fchunks = (fwords + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
@@ -1467,6 +1820,19 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				if (ev)
 					cudaEventRecord(ev[j], c.stream);
 			};
+			if (gsmall)
+			{
+				const uint32_t lm = tn.lane_max;
+				if (lm == 8)
+					launch_small_rounds<8>(c.stream, gsmall, ctl, bar, fr, c.dtris, c.dsrc, c.dE, inc, Kw, S, R, T,
+										   small_max);
+				else if (lm == 32)
+					launch_small_rounds<32>(c.stream, gsmall, ctl, bar, fr, c.dtris, c.dsrc, c.dE, inc, Kw, S, R, T,
+											small_max);
+				else
+					launch_small_rounds<THREAD_MODE_MAX>(c.stream, gsmall, ctl, bar, fr, c.dtris, c.dsrc, c.dE, inc,
+														 Kw, S, R, T, small_max);
+			}
 			tick(0);
 			k_gather_next<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, fr);
 			tick(1);
@@ -1521,13 +1887,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			if (ev)
 				cudaEventRecord(ev[PROF_STEPS], c.stream);
 		};
-		const uint32_t per_round = (flags ? 8u : 6u) + (fbits ? 4u : 0u);
-		// Rounds are replayed from a CUDA graph of rpr rounds; the host reads
-		// the control block once per replay. Rounds after the last one are
-		// no-ops.
-		cudaGraph_t graph = nullptr;
-		cudaGraphExec_t exec = nullptr;
-		bool use_graph = !profile && cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+		const uint32_t per_round = (flags ? 8u : 6u) + (fbits ? 4u : 0u) + (gsmall ? 1u : 0u);
 		const uint32_t gcompact = grid_for(c, c.m, PEEL_THREADS / 32, 16);
 		// after every rpr rounds: the gated in-place compaction
 		const bool compaction = flags && compact_div != 0;
@@ -1539,6 +1899,83 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 																	  inc.tpos);
 		};
 		const uint32_t per_replay = compaction ? 2u : 0u;
+		// Bounds of the peel: every round that is not a no-op peels at least
+		// one triangle, so T + 1 rounds suffice; the bound leaves a wide margin.
+		const uint64_t max_rounds = 2 * T + 4096;
+		const uint32_t max_rounds32 = uint32_t(std::min<uint64_t>(max_rounds, 0xfffffff0ull));
+		const unsigned long long limit_ns = (c.opt_flags & NUCLEUS34_OPT_PROFILE_PEEL) ? ~0ull : PEEL_TIME_LIMIT_NS;
+		uint64_t rounds = 0;
+		// Device loop: one CUDA graph whose while node repeats a body of rpr
+		// rounds, the compaction and k_loop_cond, which ends the loop when the
+		// peel is done, a device check failed, or a bound was reached. The host
+		// launches it once and waits once: no host round trip between rounds.
+		cudaGraph_t loop_graph = nullptr;
+		cudaGraphExec_t loop_exec = nullptr;
+		bool device_loop = false;
+		if (!profile && !(c.opt_flags & NUCLEUS34_OPT_HOST_LOOP))
+		{
+			cudaGraphConditionalHandle cond{};
+			cudaGraphNodeParams cp{};
+			cudaGraphNode_t cnode = nullptr;
+			if (cudaGraphCreate(&loop_graph, 0) == cudaSuccess &&
+				cudaGraphConditionalHandleCreate(&cond, loop_graph, 1, cudaGraphCondAssignDefault) == cudaSuccess)
+			{
+				cp.type = cudaGraphNodeTypeConditional;
+				cp.conditional.handle = cond;
+				cp.conditional.type = cudaGraphCondTypeWhile;
+				cp.conditional.size = 1;
+				if (cudaGraphAddNode(&cnode, loop_graph, nullptr, 0, &cp) == cudaSuccess &&
+					cudaStreamBeginCaptureToGraph(c.stream, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+												  cudaStreamCaptureModeThreadLocal) == cudaSuccess)
+				{
+					for (uint32_t r = 0; r < rpr; ++r)
+						launch_round(nullptr, nullptr);
+					launch_compaction();
+					k_loop_cond<<<1, 1, 0, c.stream>>>(ctl, cond, max_rounds32, limit_ns);
+					cudaGraph_t body = nullptr;
+					device_loop = cudaStreamEndCapture(c.stream, &body) == cudaSuccess &&
+								  cudaGraphInstantiate(&loop_exec, loop_graph, 0) == cudaSuccess;
+				}
+			}
+			cudaGetLastError();
+			if (!device_loop)
+			{
+				if (loop_exec)
+					cudaGraphExecDestroy(loop_exec);
+				loop_exec = nullptr;
+			}
+		}
+		if (device_loop)
+		{
+			if (cudaGraphLaunch(loop_exec, c.stream) != cudaSuccess ||
+				cudaStreamSynchronize(c.stream) != cudaSuccess)
+				rc = fail(NUCLEUS34_E_CUDA, std::string("peel device loop: ") + cudaGetErrorString(cudaGetLastError()));
+			CtlX hx{};
+			if (!rc && cudaMemcpy(&hx, ctl, sizeof(CtlX), cudaMemcpyDeviceToHost) != cudaSuccess)
+				rc = fail(NUCLEUS34_E_CUDA, "peel control");
+			if (!rc)
+			{
+				rounds = hx.c.round;
+				c.launches += (uint64_t(rounds + rpr - 1) / rpr) * (uint64_t(rpr) * per_round + per_replay + 1);
+				if (hx.timed_out || (!hx.c.done && !hx.c.error))
+					rc = fail(NUCLEUS34_E_TIMEOUT, "peel did not converge within its round and time bounds");
+			}
+			cudaGraphExecDestroy(loop_exec);
+			cudaGraphDestroy(loop_graph);
+			loop_graph = nullptr;
+			if (rc)
+				break;
+		}
+		if (loop_graph)
+			cudaGraphDestroy(loop_graph);
+		// Host loop (profiling, or where the device loop could not be built):
+		// rounds are replayed from a CUDA graph of rpr rounds; the host reads
+		// the control block once per replay. Rounds after the last one are
+		// no-ops.
+		cudaGraph_t graph = nullptr;
+		cudaGraphExec_t exec = nullptr;
+		bool use_graph = !device_loop && !profile &&
+						 cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
 		if (use_graph)
 		{
 			for (uint32_t r = 0; r < rpr; ++r)
@@ -1562,18 +1999,15 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			for (auto &e : events)
 				cudaEventCreate(&e);
 		}
-		// Bounded host loop: every round that is not a no-op peels at least one
-		// triangle, so T + 1 rounds suffice; the bound leaves a wide margin.
 		// The next replay is queued before the host reads the control block of
 		// the previous one (pinned ring of two), so the GPU never waits on the
 		// host; after the last round the queued replay is all no-ops.
-		const uint64_t max_rounds = 2 * T + 4096;
-		uint64_t rounds = 0;
 		PeelCtl *ring = nullptr;
 		cudaEvent_t ring_ev[2] = {nullptr, nullptr};
-		if (cudaMallocHost(&ring, 2 * sizeof(PeelCtl)) != cudaSuccess ||
-			cudaEventCreateWithFlags(&ring_ev[0], cudaEventDisableTiming) != cudaSuccess ||
-			cudaEventCreateWithFlags(&ring_ev[1], cudaEventDisableTiming) != cudaSuccess)
+		if (!device_loop &&
+			(cudaMallocHost(&ring, 2 * sizeof(PeelCtl)) != cudaSuccess ||
+			 cudaEventCreateWithFlags(&ring_ev[0], cudaEventDisableTiming) != cudaSuccess ||
+			 cudaEventCreateWithFlags(&ring_ev[1], cudaEventDisableTiming) != cudaSuccess))
 			rc = fail(NUCLEUS34_E_CUDA, "peel control ring");
 		auto enqueue = [&](int slot) -> bool {
 			if (use_graph)
@@ -1597,13 +2031,13 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 		// profiling reads per-round events, so it runs one replay at a time
 		const int depth = profile ? 1 : 2;
 		uint64_t issued = 0, consumed = 0;
-		while (!rc && issued < uint64_t(depth))
+		while (!rc && !device_loop && issued < uint64_t(depth))
 		{
 			if (!enqueue(int(issued & 1)))
 				rc = fail(NUCLEUS34_E_CUDA, "peel replay launch");
 			++issued;
 		}
-		while (!rc)
+		while (!rc && !device_loop)
 		{
 			const int slot = int(consumed & 1);
 			if (cudaEventSynchronize(ring_ev[slot]) != cudaSuccess || cudaGetLastError() != cudaSuccess)
@@ -1699,6 +2133,11 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			cudaStreamSynchronize(c.stream) != cudaSuccess)
 		{
 			rc = fail(NUCLEUS34_E_CUDA, "peel stats");
+			break;
+		}
+		if (hctl->error & 4u)
+		{
+			rc = fail(NUCLEUS34_E_TIMEOUT, "peel: a grid barrier of the small-round kernel ran past its time bound");
 			break;
 		}
 		if (hctl->error)

@@ -389,6 +389,8 @@ OPT_PROFILE_PEEL = 0x2
 OPT_LEAN_MEMORY = 0x4
 OPT_VERIFIABLE = 0x8
 OPT_HOST_RESULTS = 0x10
+OPT_HOST_LOOP = 0x20
+OPT_NO_SMALL_ROUNDS = 0x40
 
 
 def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1, flags: int = 0,

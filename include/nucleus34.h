@@ -98,6 +98,19 @@ typedef struct
  * chosen automatically when the next pass would not fit beside the results
  * kept on the device. Results and accessors are unchanged. */
 #define NUCLEUS34_OPT_HOST_RESULTS 0x10u
+/* opts.flags: drive the peel rounds from the host (a CUDA graph of a fixed
+ * number of rounds replayed, the host reading the control block after each
+ * replay) instead of the default device loop (one CUDA graph whose while
+ * node repeats the rounds until the peel is done, launched once). Results
+ * are identical; kept for comparison and for drivers without conditional
+ * graph nodes. */
+#define NUCLEUS34_OPT_HOST_LOOP 0x20u
+/* opts.flags: run every peel round as separate kernel launches, instead of
+ * running consecutive small cascade rounds (at most 8192 dying triangles, no
+ * level change) inside one cooperative launch with grid barriers between the
+ * steps of a round (the default for the on-demand peel with death flags).
+ * Results are identical; kept for comparison. */
+#define NUCLEUS34_OPT_NO_SMALL_ROUNDS 0x40u
 
 typedef struct
 {

@@ -130,3 +130,47 @@ def test_lean_and_profiled_peels_match(n34, oracle, case):
     prof = n34.decompose(g, variant="ondemand", flags=n34.OPT_PROFILE_PEEL)
     assert np.array_equal(prof.k, o.k)
     assert prof.result["t_peel_debit"] > 0
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("flags", [0x0, 0x4, 0x1])
+def test_device_loop_and_host_loop_agree(n34, oracle, variant, flags):
+    """The default device loop (one CUDA graph whose while node repeats the
+    rounds) and the host-driven replay loop give the oracle's k, in the
+    regular, memory-lean and round-stamp peels."""
+    if variant == "direct" and flags:
+        pytest.skip("the layout flags concern the on-demand peel")
+    s, t = n34.gen_rmat(12, 16, 4)
+    g = n34.graph_from_edges(s, t)
+    o = oracle.decompose(g)
+    dev = n34.decompose(g, variant=variant, flags=flags)
+    host = n34.decompose(g, variant=variant, flags=flags | n34.OPT_HOST_LOOP)
+    assert np.array_equal(dev.k, o.k) and np.array_equal(host.k, o.k)
+    assert dev.result["peeling_iterations"] == host.result["peeling_iterations"]
+
+
+def test_listing_chunks_match_one_pass(n34, oracle):
+    """With the listing's bit words capped (NUCLEUS34_LIST_CHUNK_WORDS, read
+    per call) it counts every chunk of sources first and repeats each chunk's
+    bits before its writes; the canonical list is the same, for chunks of
+    many sources and for chunks of one."""
+    import subprocess
+    import sys
+    code = ("import sys, json, hashlib; sys.path.insert(0, sys.argv[1]); import nucleus34 as n34\n"
+            "s, t = n34.gen_rmat(13, 16, 6); g = n34.graph_from_edges(s, t)\n"
+            "d = n34.decompose(g, variant='ondemand', n_quds=0)\n"
+            "print(json.dumps([hashlib.sha256(d.tris.tobytes()).hexdigest(), "
+            "hashlib.sha256(d.k.tobytes()).hexdigest()]))\n")
+    s, t = n34.gen_rmat(13, 16, 6)
+    o = oracle.decompose(n34.graph_from_edges(s, t))
+    import hashlib
+    import json
+    import os
+    want = [hashlib.sha256(o.tris.astype(np.uint32).tobytes()).hexdigest(),
+            hashlib.sha256(o.k.astype(np.int32).tobytes()).hexdigest()]
+    pkg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "gpu-nucleus34_b200")
+    for cap in ("4096", "1"):
+        env = dict(os.environ, NUCLEUS34_LIST_CHUNK_WORDS=cap)
+        r = subprocess.run([sys.executable, "-c", code, pkg], capture_output=True, text=True, timeout=300, env=env)
+        assert r.returncode == 0, r.stderr[-2000:]
+        assert json.loads(r.stdout.strip().splitlines()[-1]) == want, cap
