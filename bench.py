@@ -74,6 +74,11 @@ def parse():
     p.add_argument("--serve-master-seed", type=int, default=5)
     p.add_argument("--serve-load", default="0.5,1,2,4",
                    help="arrival rates as multiples of the serial plain capacity")
+    p.add_argument("--serve-route", default="memory", choices=["memory", "ondemand"],
+                   help="variant per request: by memory estimate (direct when it fits budget/direct_div) or on-demand")
+    p.add_argument("--serve-direct-div", type=int, default=0)
+    p.add_argument("--serve-budget-gb", type=float, default=0.0, help="server memory budget (0: the device's)")
+    p.add_argument("--serve-workers", type=int, default=2)
     p.add_argument("--batch-master-seed", type=int, default=4)
     return p.parse_args()
 
@@ -267,27 +272,59 @@ def batch_specs(count, master):
     return out
 
 
+def replica_setup():
+    """(rank, world, local device, dist module or None) for replicas under
+    torchrun: one process per GPU, NCCL only for the barrier and the
+    max-over-ranks timing (the graphs are independent: no data collective)."""
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world <= 1:
+        return 0, 1, local, None
+    import torch.distributed as tdist
+    from datetime import timedelta
+    tdist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    return rank, world, local, tdist
+
+
+def my_share(n34, graphs, rank, world):
+    """Indices of the graphs this rank decomposes (nucleus34_split_plan by
+    estimated cost; every rank derives the same plan)."""
+    if world <= 1:
+        return list(range(len(graphs)))
+    part_of, _ = n34.split_plan([n34.graph_cost(g) for g in graphs], world)
+    return [i for i in range(len(graphs)) if part_of[i] == rank]
+
+
 def run_batch(a):
     """Batched form: one nucleus34_batch_decompose pass over all graphs against
     one nucleus34_ctx_upload + nucleus34_ctx_run per graph on the same GPU;
-    every graph's k compared bit for bit."""
+    every graph's k compared bit for bit. Under torchrun each rank takes its
+    share of the graphs (replicas); times are the slowest rank's."""
     import numpy as np
     import torch
     import nucleus34 as n34
-    torch.cuda.set_device(0)
+    rank, world, dev, tdist = replica_setup()
     t0 = time.perf_counter()
     graphs = []
     for kind, x, y, seed in batch_specs(a.batch_graphs, a.batch_master_seed):
         src, dst = n34.gen_rmat(x, y, seed) if kind == "rmat" else n34.gen_ws(x, y, 0.1, seed)
         graphs.append(n34.graph_from_edges(src, dst))
-    log(f"[bench] generated {len(graphs)} graphs in {time.perf_counter() - t0:.1f} s, "
+    n_all = len(graphs)
+    share = my_share(n34, graphs, rank, world)
+    graphs = [graphs[i] for i in share]
+    log(f"[bench] rank {rank}: {len(graphs)} of {n_all} graphs in {time.perf_counter() - t0:.1f} s, "
         f"{sum(g.m for g in graphs)} oriented edges")
     # plain: one decomposition per graph (context reused, graph uploaded each time)
     plain_k, plain_dev = [], 0.0
-    with n34.Context() as ctx:
+    with n34.Context(device=dev) as ctx:
         ctx.upload(graphs[0])
         ctx.run("ondemand")  # warm-up
         torch.cuda.synchronize()
+        if tdist:
+            tdist.barrier()
         w0 = time.perf_counter()
         for g in graphs:
             ctx.upload(g)
@@ -296,11 +333,13 @@ def run_batch(a):
             plain_k.append(ctx.copy_k(int(r["triangle_count"])))
         plain_wall = time.perf_counter() - w0
     # batched: warm-up pass, then the timed pass
-    with n34.batch_decompose(graphs[: min(64, len(graphs))]):
+    with n34.batch_decompose(graphs[: min(64, len(graphs))], device=dev):
         pass
     torch.cuda.synchronize()
+    if tdist:
+        tdist.barrier()
     w0 = time.perf_counter()
-    b = n34.batch_decompose(graphs)
+    b = n34.batch_decompose(graphs, device=dev)
     batch_wall = time.perf_counter() - w0
     res = b.result
     mism = 0
@@ -308,9 +347,19 @@ def run_batch(a):
         if not np.array_equal(b.copy_k(i), plain_k[i]):
             mism += 1
     b.close()
-    n = len(graphs)
+    if tdist:
+        batch_wall = max_over_ranks(batch_wall, f"cuda:{dev}")
+        plain_wall = max_over_ranks(plain_wall, f"cuda:{dev}")
+        plain_dev = max_over_ranks(plain_dev, f"cuda:{dev}")
+        mism = int(max_over_ranks(float(mism), f"cuda:{dev}"))
+        tdist.barrier()
+        tdist.destroy_process_group()
+        if rank != 0:
+            return 0
+    n = n_all
     line = {
-        "metric": "graphs/s (batched form)", "value": n / batch_wall, "unit": "graphs/s", "n_gpus": 1,
+        "metric": "graphs/s (batched form)", "value": n / batch_wall, "unit": "graphs/s", "n_gpus": world,
+        "scaling": "strong", "parallelism": f"replicas x{world}: graphs split by nucleus34_split_plan, no collective",
         "higher_is_better": True, "dtype": "int32", "data": "synthetic (seeded R-MAT + Watts-Strogatz)",
         "config": {"workload": f"{n} graphs: half R-MAT scale 8..14 ef 8..24, half Watts-Strogatz n 500..20000 "
                                f"k=10 beta=0.1, master seed {a.batch_master_seed}",
@@ -353,82 +402,114 @@ def serve_specs(count, master, max_edges):
 
 def run_serve(a):
     """Serving: Poisson arrivals into nucleus34_server (continuous batching,
-    two workers) against serial plain execution (one decomposition per request,
-    FIFO, same arrival times: latencies from the measured service times)."""
+    variant chosen per request by its memory estimate) against serial plain
+    execution (one on-demand decomposition per request, FIFO, same arrival
+    times: latencies from the measured service times). Under torchrun each
+    rank serves its share of the requests (nucleus34_split_plan) on its own
+    GPU with the same arrival times; latencies are gathered on rank 0."""
     import numpy as np
     import torch
     import nucleus34 as n34
-    torch.cuda.set_device(0)
+    rank, world, dev, tdist = replica_setup()
     t0 = time.perf_counter()
     graphs = []
     for kind, x, y, seed in serve_specs(a.serve_requests, a.serve_master_seed, a.serve_max_edges):
         src, dst = n34.gen_rmat(x, y, seed) if kind == "rmat" else n34.gen_rgg(x, y, seed)
         graphs.append(n34.graph_from_edges(src, dst))
-    n = len(graphs)
-    log(f"[bench] generated {n} requests in {time.perf_counter() - t0:.1f} s, "
-        f"{sum(g.m for g in graphs)} oriented edges")
-    # serial plain service times (and the reference results)
-    service, alone_k = [], []
-    with n34.Context() as ctx:
-        ctx.upload(graphs[0])
+    n_all = len(graphs)
+    share = my_share(n34, graphs, rank, world)
+    log(f"[bench] rank {rank}: {len(share)} of {n_all} requests in {time.perf_counter() - t0:.1f} s, "
+        f"{sum(graphs[i].m for i in share)} oriented edges")
+    route = n34.ROUTE_MEMORY if a.serve_route == "memory" else n34.ROUTE_ONDEMAND
+    budget = int(a.serve_budget_gb * 1e9)
+    # serial plain service times (and the reference results) of this rank's share
+    service, alone_k = {}, {}
+    with n34.Context(device=dev) as ctx:
+        ctx.upload(graphs[share[0]])
         ctx.run("ondemand")
-        for g in graphs:
+        for i in share:
             w = time.perf_counter()
-            ctx.upload(g)
+            ctx.upload(graphs[i])
             r = ctx.run("ondemand")
             k = ctx.copy_k(int(r["triangle_count"]))
-            service.append(time.perf_counter() - w)
-            alone_k.append(k)
-    cap = n / sum(service)  # serial plain capacity, requests/s
+            service[i] = time.perf_counter() - w
+            alone_k[i] = k
+    tot_service = sum(service.values())
+    if tdist:
+        tot_service = max_over_ranks(tot_service, f"cuda:{dev}")
+    cap = n_all / tot_service  # plain capacity of the job (each rank serially), requests/s
     rng = np.random.default_rng(a.serve_master_seed)
-    gaps = rng.exponential(1.0, n)
+    gaps = rng.exponential(1.0, n_all)
     sweeps = []
     mism = 0
     for load in [float(x) for x in a.serve_load.split(",")]:
         rate = load * cap
         arr = np.cumsum(gaps / rate)
-        # serial plain: FIFO single server
-        done, lat = 0.0, []
-        for i in range(n):
+        # serial plain: FIFO single server per rank
+        done, lat_plain = 0.0, []
+        for i in share:
             start = max(arr[i], done)
             done = start + service[i]
-            lat.append(done - arr[i])
-        plain = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                 "graphs_per_s": n / (done - arr[0])}
+            lat_plain.append(done - arr[i])
+        plain_end = done - arr[0]
         # the server, fed in real time
-        with n34.Server(workers=2) as srv:
-            ids = [0] * n
+        if tdist:
+            tdist.barrier()
+        with n34.Server(device=dev, mem_budget_bytes=budget, workers=a.serve_workers, route=route,
+                        direct_div=a.serve_direct_div) as srv:
+            ids = {}
             w0 = time.perf_counter()
-            for i in range(n):
+            for i in share:
                 wait = arr[i] - arr[0] - (time.perf_counter() - w0)
                 if wait > 0:
                     time.sleep(wait)
                 ids[i] = srv.submit(graphs[i])
-            infos = [srv.wait(rid) for rid in ids]
+            infos = {i: srv.wait(rid) for i, rid in ids.items()}
             end = time.perf_counter() - w0
-            for i, (rid, info) in enumerate(zip(ids, infos)):
-                if not np.array_equal(srv.copy_k(rid, info["triangle_count"]), alone_k[i]):
+            for i, rid in ids.items():
+                if not np.array_equal(srv.copy_k(rid, infos[i]["triangle_count"]), alone_k[i]):
                     mism += 1
             st = srv.stats()
-        slat = [x["latency_seconds"] for x in infos]
-        worst = sorted(range(n), key=lambda i: -slat[i])[:8]
-        log(f"[bench] load {load}: slowest requests (latency, queue, triangles, pass, arrival): " +
-            "; ".join(f"{slat[i]:.3f} {infos[i]['queue_seconds']:.3f} {infos[i]['triangle_count']} "
-                      f"{infos[i]['pass']} {arr[i] - arr[0]:.2f}" for i in worst))
-        served = {"p50_s": float(np.percentile(slat, 50)), "p99_s": float(np.percentile(slat, 99)),
-                  "graphs_per_s": n / end, "passes": int(st["passes"])}
+        slat = [infos[i]["latency_seconds"] for i in share]
+        ndirect = sum(1 for i in share if infos[i]["direct"])
+        worst = sorted(share, key=lambda i: -infos[i]["latency_seconds"])[:8]
+        log(f"[bench] rank {rank} load {load}: slowest requests (latency, queue, triangles, pass, arrival, direct): " +
+            "; ".join(f"{infos[i]['latency_seconds']:.3f} {infos[i]['queue_seconds']:.3f} "
+                      f"{infos[i]['triangle_count']} {infos[i]['pass']} {arr[i] - arr[0]:.2f} {int(infos[i]['direct'])}"
+                      for i in worst))
+        mine = {"slat": slat, "plat": lat_plain, "end": end, "plain_end": plain_end, "passes": int(st["passes"]),
+                "direct": ndirect}
+        parts = [mine]
+        if tdist:
+            parts = [None] * world
+            tdist.all_gather_object(parts, mine)
+        slat_all = [x for p in parts for x in p["slat"]]
+        plat_all = [x for p in parts for x in p["plat"]]
+        end_all = max(p["end"] for p in parts)
+        plain = {"p50_s": float(np.percentile(plat_all, 50)), "p99_s": float(np.percentile(plat_all, 99)),
+                 "graphs_per_s": n_all / max(p["plain_end"] for p in parts)}
+        served = {"p50_s": float(np.percentile(slat_all, 50)), "p99_s": float(np.percentile(slat_all, 99)),
+                  "graphs_per_s": n_all / end_all, "passes": sum(p["passes"] for p in parts),
+                  "direct_requests": sum(p["direct"] for p in parts)}
         sweeps.append({"load": load, "rate_per_s": rate, "server": served, "serial_plain": plain})
         log(f"[bench] load {load}: server p50 {served['p50_s']:.3f} p99 {served['p99_s']:.3f} "
-            f"{served['graphs_per_s']:.1f}/s ({served['passes']} passes); plain p50 {plain['p50_s']:.3f} "
-            f"p99 {plain['p99_s']:.3f} {plain['graphs_per_s']:.1f}/s")
+            f"{served['graphs_per_s']:.1f}/s ({served['passes']} passes, {served['direct_requests']} direct); "
+            f"plain p50 {plain['p50_s']:.3f} p99 {plain['p99_s']:.3f} {plain['graphs_per_s']:.1f}/s")
+    if tdist:
+        mism = int(max_over_ranks(float(mism), f"cuda:{dev}"))
+        tdist.barrier()
+        tdist.destroy_process_group()
+        if rank != 0:
+            return 0
     top = sweeps[-1]
     line = {
         "metric": "graphs/s and p50/p99 latency (serving)", "value": top["server"]["graphs_per_s"],
-        "unit": "graphs/s", "n_gpus": 1, "higher_is_better": True, "dtype": "int32",
+        "unit": "graphs/s", "n_gpus": world, "higher_is_better": True, "dtype": "int32", "scaling": "strong",
         "data": "synthetic (seeded R-MAT + 2D random geometric graphs)",
-        "config": {"workload": f"{n} requests, Poisson arrivals, half R-MAT half RGG (degree 16..64), undirected "
+        "config": {"workload": f"{n_all} requests, Poisson arrivals, half R-MAT half RGG (degree 16..64), undirected "
                                f"edges log-uniform 1e3..{a.serve_max_edges:.0e}, master seed {a.serve_master_seed}",
-                   "serial_plain_capacity_per_s": cap},
+                   "serial_plain_capacity_per_s": cap, "route": a.serve_route, "workers": a.serve_workers,
+                   "budget_bytes": budget or "device", "parallelism": f"replicas x{world}"},
         "sweep": sweeps, "k_mismatched_requests": mism,
     }
     print(json.dumps(line), flush=True)

@@ -7,9 +7,9 @@
 //
 // Here: per-edge counts (atomics) -> exclusive scan -> scatter of 64-bit
 // (x<<32 | t) entries into their edge's segment -> a segmented sort of each
-// segment by x (segments are short: a warp bitonic network for <= 32 entries,
-// a shared-memory block bitonic sort up to SEG_SMEM, a global-memory bitonic
-// sort on a padded copy beyond that) -> split into the third[] and tri[]
+// segment by x (segments are short: a warp bitonic network on registers for
+// <= 256 entries, a shared-memory block bitonic sort up to SEG_SMEM, a
+// global-memory bitonic sort on a padded copy beyond that) -> split into the third[] and tri[]
 // arrays the 3-way intersection reads. Triangle t = (a,b,c) with u = src[b],
 // v = E[b], w = E[c] is listed under b with x = w, under a with x = v and under
 // c with x = u, exactly the reference's three entries.
@@ -21,6 +21,7 @@ namespace n34 {
 
 namespace {
 
+constexpr int SEG_WARP_MAX = 256;     // keys per warp sort (8 registers per lane)
 constexpr int SEG_SMEM = 8192;        // keys per block sort (64 KB smem)
 constexpr int SEG_BLOCK = 512;
 
@@ -95,7 +96,7 @@ __global__ void k_seg_classify(const uint64_t *__restrict__ incO, uint64_t m, ui
 		uint64_t len = 0;
 		if (e < m)
 			len = incO[e + 1] - incO[e];
-		const int cls = len < 2 ? -1 : (len <= 32 ? 0 : (len <= SEG_SMEM ? 1 : 2));
+		const int cls = len < 2 ? -1 : (len <= SEG_WARP_MAX ? 0 : (len <= SEG_SMEM ? 1 : 2));
 #pragma unroll
 		for (int k = 0; k < 3; ++k)
 		{
@@ -108,34 +109,96 @@ __global__ void k_seg_classify(const uint64_t *__restrict__ incO, uint64_t m, ui
 	}
 }
 
-// Warp per segment (<= 32 entries): register bitonic network.
+// Bitonic network over 32*K keys held K per lane (element k*32 + lane in
+// v[k]): strides below 32 pair lanes (shuffles), larger ones pair registers
+// of the same lane.
+template <int K>
+__device__ __forceinline__ void warp_bitonic(unsigned long long (&v)[K])
+{
+	const uint32_t lane = lane_id();
+#pragma unroll
+	for (uint32_t size = 2; size <= 32u * K; size <<= 1)
+	{
+#pragma unroll
+		for (uint32_t stride = size >> 1; stride > 0; stride >>= 1)
+		{
+			if (stride >= 32)
+			{
+				const uint32_t ks = stride >> 5;
+#pragma unroll
+				for (int k = 0; k < K; ++k)
+				{
+					if ((uint32_t(k) & ks) == 0)
+					{
+						const int k2 = int(uint32_t(k) | ks);
+						const bool up = ((uint32_t(k) * 32 + lane) & size) == 0;
+						const unsigned long long a = v[k], b = v[k2];
+						if ((a > b) == up)
+						{
+							v[k] = b;
+							v[k2] = a;
+						}
+					}
+				}
+			}
+			else
+			{
+#pragma unroll
+				for (int k = 0; k < K; ++k)
+				{
+					const unsigned long long o = __shfl_xor_sync(FULL, v[k], stride);
+					const bool up = ((uint32_t(k) * 32 + lane) & size) == 0;
+					const bool lower = (lane & stride) == 0;
+					const unsigned long long mn = v[k] < o ? v[k] : o, mx = v[k] < o ? o : v[k];
+					v[k] = (lower == up) ? mn : mx;
+				}
+			}
+		}
+	}
+}
+
+template <int K>
+__device__ __forceinline__ void warp_sort_segment(const EntryStore &keys, uint64_t b, uint32_t len)
+{
+	const uint32_t lane = lane_id();
+	unsigned long long v[K];
+#pragma unroll
+	for (int k = 0; k < K; ++k)
+	{
+		const uint32_t i = uint32_t(k) * 32 + lane;
+		v[k] = i < len ? keys.ld(b + i) : ~0ull;
+	}
+	warp_bitonic<K>(v);
+#pragma unroll
+	for (int k = 0; k < K; ++k)
+	{
+		const uint32_t i = uint32_t(k) * 32 + lane;
+		if (i < len)
+			keys.st(b + i, v[k]);
+	}
+}
+
+// Warp per segment (<= SEG_WARP_MAX entries): register bitonic network of
+// the smallest power of two that holds it.
 __global__ void k_seg_sort_warp(const uint32_t *__restrict__ list, const uint32_t *__restrict__ count,
 								const uint64_t *__restrict__ incO, EntryStore keys)
 {
 	const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
 	const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
 	const uint32_t n = *count;
-	const uint32_t lane = lane_id();
 	for (uint64_t i = warp; i < n; i += nwarps)
 	{
 		const uint32_t e = list[i];
-		const uint64_t b = incO[e], len = incO[e + 1] - b;
-		unsigned long long k = lane < len ? keys.ld(b + lane) : ~0ull;
-#pragma unroll
-		for (int size = 2; size <= 32; size <<= 1)
-		{
-#pragma unroll
-			for (int stride = size >> 1; stride > 0; stride >>= 1)
-			{
-				const unsigned long long o = __shfl_xor_sync(FULL, k, stride);
-				const bool up = (lane & size) == 0;
-				const bool lower = (lane & stride) == 0;
-				const unsigned long long mn = k < o ? k : o, mx = k < o ? o : k;
-				k = (lower == up) ? mn : mx;
-			}
-		}
-		if (lane < len)
-			keys.st(b + lane, k);
+		const uint64_t b = incO[e];
+		const uint32_t len = uint32_t(incO[e + 1] - b);
+		if (len <= 32)
+			warp_sort_segment<1>(keys, b, len);
+		else if (len <= 64)
+			warp_sort_segment<2>(keys, b, len);
+		else if (len <= 128)
+			warp_sort_segment<4>(keys, b, len);
+		else
+			warp_sort_segment<8>(keys, b, len);
 	}
 }
 

@@ -1,18 +1,29 @@
 // Serving: a request loop that keeps graph state on the device and batches
 // requests continuously (nucleus34_server_*).
 //
-// Each worker owns a context (device, stream, pooled memory). A worker takes
-// the pending requests in arrival order that fit the memory still free in the
-// budget (estimated per request from its CSR) and within the 32-bit entry
-// range, decomposes them in one pass as a disjoint union (the batched form),
-// copies every request's results to the host and signals it. Requests that
-// arrive while passes run are admitted by the next free worker, so with two
-// or more workers their passes overlap on the device. A request that asks
-// for its four-clique list is routed to the direct variant and runs alone.
-// Results do not depend on the mix: a graph's triangles and k in a union
-// equal those of the graph alone (the batched form's argument).
+// Each worker owns a context (device, stream, pooled memory) on one device
+// slot; a slot is a device with its own memory budget, and several slots may
+// name one GPU. A worker takes the pending requests in arrival order that fit
+// the memory still free in its slot (estimated per request from its CSR) and
+// within the 32-bit ranges, decomposes them in one pass as a disjoint union
+// (the batched form), copies every request's results to the host and signals
+// it. Requests that arrive while passes run are admitted by the next free
+// worker, so with two or more workers their passes overlap on the device.
 //
-// The reference has no serving loop; it runs one graph per process.
+// Routing. Each request's variant is fixed at submission by its memory
+// estimate: the direct variant (four-clique list kept and peeled by clique
+// ids) when its estimate is at most 1/direct_div of a slot's budget, the
+// on-demand variant (cliques re-enumerated) otherwise; a request for its
+// clique list is always direct. The direct estimate counts out-triples
+// sum_u C(d+(u), 3), which bound the four-cliques (every four-clique has one
+// lowest vertex in the orientation with the other three among its
+// out-neighbours); a direct union is cut so that this bound stays below
+// 2^32, the direct variant's clique-id range. This generalises the
+// reference's projection of the direct peel's memory (cuNucleus34.cu:563-585),
+// which reports whether that peel will fit but does not choose.
+//
+// Results do not depend on the mix: a graph's triangles, cliques and k in a
+// union equal those of the graph alone (the batched form's argument).
 #include "pipeline.cuh"
 
 #include <algorithm>
@@ -44,8 +55,10 @@ struct Request
 	// owned copy of the CSR
 	uint64_t n = 0, m = 0;
 	std::vector<uint32_t> O, D, E;
-	uint64_t est_bytes = 0;     // admission estimate of the pass memory it needs
-	uint64_t est_triangles = 0; // upper bound (wedges)
+	uint64_t est_bytes = 0;     // admission estimate of the pass memory it needs (its variant)
+	uint64_t est_triangles = 0; // upper bound (out-wedges)
+	uint64_t est_cliques = 0;   // upper bound (out-triples)
+	bool direct = false;        // variant chosen at submission
 	// result
 	bool done = false;
 	int status = NUCLEUS34_OK;
@@ -59,40 +72,63 @@ struct Request
 };
 
 // Bytes of one pass per triangle (peak: listing, incidence build, support,
-// peel arrays) and per oriented edge (CSR, sources, spans, counts).
+// peel arrays) and per oriented edge (CSR, sources, spans, counts); the
+// direct variant adds its clique list and triangle->clique incidence (16 +
+// 16 bytes per clique) and one destroyed flag per clique. Applied to the
+// out-wedge and out-triple bounds, not to the true counts, so they
+// overestimate; tests/test_server.py checks them against measured peaks.
 constexpr uint64_t PASS_BYTES_PER_TRIANGLE = 80;
 constexpr uint64_t PASS_BYTES_PER_EDGE = 40;
-constexpr uint64_t DIRECT_BYTES_PER_WEDGE = 96; // clique list + incidence, per wedge bound
+constexpr uint64_t DIRECT_BYTES_PER_CLIQUE = 33;
+constexpr uint32_t DEFAULT_DIRECT_DIV = 8;
+
+struct Slot
+{
+	int device = 0;
+	uint64_t budget = 0;
+	uint64_t in_flight = 0;
+};
 
 } // namespace
 
 struct nucleus34_server_s
 {
 	nucleus34_opts opts{};
-	uint64_t budget = 0;          // bytes shared by all passes in flight
+	std::vector<Slot> slots;      // device slots, each with its own budget
 	uint64_t max_batch = 256;     // graphs per pass
+	uint32_t route = NUCLEUS34_ROUTE_MEMORY;
+	uint32_t direct_div = DEFAULT_DIRECT_DIV;
 	std::mutex mu;
 	std::condition_variable cv_work, cv_done;
 	std::deque<std::shared_ptr<Request>> pending;
 	std::map<uint64_t, std::shared_ptr<Request>> all;
-	uint64_t next_id = 1, in_flight_bytes = 0, passes = 0, served = 0, busy_workers = 0;
+	uint64_t next_id = 1, passes = 0, served = 0, direct_served = 0, busy_workers = 0;
 	bool stop = false;
 	std::vector<std::thread> workers;
-	std::vector<nucleus34_ctx> ctxs;
+	std::vector<nucleus34_ctx> ctxs;   // one per worker
+	std::vector<size_t> worker_slot;   // slot of each worker
 };
 
 namespace {
 
-uint64_t wedge_bound(const uint32_t *D, uint64_t n)
+// Out-wedges sum_u C(d, 2) (bound on the triangles) and out-triples
+// sum_u C(d, 3) (bound on the four-cliques); the triples saturate at 2^63.
+void out_bounds(const uint32_t *D, uint64_t n, uint64_t &wedges, uint64_t &triples)
 {
-	uint64_t w = 0;
+	wedges = 0;
+	triples = 0;
 	for (uint64_t u = 0; u < n; ++u)
-		w += uint64_t(D[u]) * (D[u] ? D[u] - 1 : 0) / 2;
-	return w;
+	{
+		const uint64_t d = D[u];
+		wedges += d * (d ? d - 1 : 0) / 2;
+		const unsigned __int128 t3 = d >= 3 ? (unsigned __int128)d * (d - 1) * (d - 2) / 6 : 0;
+		const unsigned __int128 sum = (unsigned __int128)triples + t3;
+		triples = sum > ((unsigned __int128)1 << 63) ? (uint64_t(1) << 63) : uint64_t(sum);
+	}
 }
 
-// one pass over a set of on-demand requests (their union) on context c
-void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch)
+// one pass over a set of requests of one variant (their union) on context c
+void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch, bool direct)
 {
 	std::vector<nucleus34_csr> csrs(batch.size());
 	for (size_t i = 0; i < batch.size(); ++i)
@@ -111,26 +147,36 @@ void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch)
 	if (!rc)
 	{
 		c.seg_eoff = eoff;
-		rc = run(c, NUCLEUS34_ONDEMAND, &r);
+		rc = run(c, direct ? NUCLEUS34_DIRECT : NUCLEUS34_ONDEMAND, &r);
 	}
-	// results to the host: k of every request, triangle lists of those that ask
-	bool want_tris = false;
+	// results to the host: k of every request, triangle and clique lists of
+	// those that ask
+	bool want_tris = false, want_quds = false;
 	for (auto &q : batch)
+	{
 		want_tris = want_tris || (q->flags & NUCLEUS34_REQ_TRIANGLES);
+		want_quds = want_quds || (q->flags & NUCLEUS34_REQ_CLIQUES);
+	}
+	want_quds = want_quds && direct;
 	std::vector<int32_t> K;
-	std::vector<uint32_t> tris;
+	std::vector<uint32_t> tris, quds;
 	if (!rc && c.T)
 	{
 		K.resize(c.T);
 		if (want_tris)
 			tris.resize(3 * c.T);
+		if (want_quds)
+			quds.resize(4 * c.Q);
 		if (cudaMemcpyAsync(K.data(), c.dK, c.T * 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
 			(want_tris &&
 			 cudaMemcpyAsync(tris.data(), c.dtris, c.T * 12, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess) ||
+			(want_quds && c.Q &&
+			 cudaMemcpyAsync(quds.data(), c.dquds, c.Q * 16, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess) ||
 			cudaStreamSynchronize(c.stream) != cudaSuccess)
 			rc = fail(NUCLEUS34_E_CUDA, "serving: result copy");
 	}
 	const std::string err = rc ? std::string(nucleus34_last_error()) : std::string();
+	uint64_t q0 = 0; // first clique of request i in the union's list (cliques are listed by lowest triangle)
 	for (size_t i = 0; i < batch.size(); ++i)
 	{
 		Request &q = *batch[i];
@@ -139,8 +185,9 @@ void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch)
 		if (rc)
 			continue;
 		const uint64_t t0 = c.seg_toff[i], T = c.seg_toff[i + 1] - t0;
+		const uint64_t Qi = c.seg_q[i];
 		q.summary.triangle_count = T;
-		q.summary.four_clique_count = c.seg_q[i];
+		q.summary.four_clique_count = Qi;
 		q.summary.k_max = c.seg_kmax[i];
 		q.summary.k_avg = T ? double(c.seg_ksum[i]) / double(T) : 0.0;
 		q.k.assign(K.begin() + t0, K.begin() + t0 + T);
@@ -151,41 +198,13 @@ void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch)
 			for (auto &x : q.tris)
 				x -= eo;
 		}
-	}
-	// a finished pass holds nothing on the device (admission counts on it)
-	c.release_results();
-	c.release_graph();
-}
-
-// a request for its clique list: the direct variant, alone
-void serve_direct(Ctx &c, Request &q)
-{
-	clear_error();
-	const nucleus34_csr u{q.n, q.m, q.O.data(), q.D.data(), q.E.empty() ? nullptr : q.E.data()};
-	int rc = upload(c, &u);
-	nucleus34_result r{};
-	if (!rc)
-		rc = run(c, NUCLEUS34_DIRECT, &r);
-	if (!rc && c.T)
-	{
-		q.k.resize(c.T);
-		q.tris.resize(3 * c.T);
-		q.quds.resize(4 * c.Q);
-		if (cudaMemcpyAsync(q.k.data(), c.dK, c.T * 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
-			cudaMemcpyAsync(q.tris.data(), c.dtris, c.T * 12, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
-			(c.Q && cudaMemcpyAsync(q.quds.data(), c.dquds, c.Q * 16, cudaMemcpyDeviceToHost, c.stream) !=
-						cudaSuccess) ||
-			cudaStreamSynchronize(c.stream) != cudaSuccess)
-			rc = fail(NUCLEUS34_E_CUDA, "serving: result copy");
-	}
-	q.status = rc;
-	q.error = rc ? std::string(nucleus34_last_error()) : std::string();
-	if (!rc)
-	{
-		q.summary.triangle_count = r.triangle_count;
-		q.summary.four_clique_count = r.four_clique_count;
-		q.summary.k_max = r.k_max;
-		q.summary.k_avg = r.k_avg;
+		if (want_quds && (q.flags & NUCLEUS34_REQ_CLIQUES))
+		{
+			q.quds.assign(quds.begin() + 4 * q0, quds.begin() + 4 * (q0 + Qi));
+			for (auto &x : q.quds)
+				x -= uint32_t(t0);
+		}
+		q0 += Qi;
 	}
 	// a finished pass holds nothing on the device (admission counts on it)
 	c.release_results();
@@ -195,8 +214,10 @@ void serve_direct(Ctx &c, Request &q)
 void worker_loop(nucleus34_server_s *s, size_t wi)
 {
 	Ctx &c = s->ctxs[wi]->c;
+	Slot &slot = s->slots[s->worker_slot[wi]];
 	cudaSetDevice(c.device);
-	const uint64_t range_limit = 0xffffffffull / 3;
+	const uint64_t range_limit = 0xffffffffull / 3; // 3T incidence entries in 32-bit positions
+	const uint64_t clique_limit = 0xffffffffull;     // direct: clique ids in 32 bits
 	for (;;)
 	{
 		std::vector<std::shared_ptr<Request>> batch;
@@ -207,54 +228,53 @@ void worker_loop(nucleus34_server_s *s, size_t wi)
 			s->cv_work.wait(lk, [&] {
 				if (s->pending.empty())
 					return s->stop;
-				// the head fits the memory left, or nothing else is running;
-				// while stopping too, so that the queued requests are finished
-				// under the same budget (a running pass always ends and wakes
-				// the waiting workers)
-				const uint64_t free_b = s->budget > s->in_flight_bytes ? s->budget - s->in_flight_bytes : 0;
-				return s->pending.front()->est_bytes <= free_b || s->in_flight_bytes == 0;
+				// the head fits the memory left in this slot, or nothing else
+				// runs there; while stopping too, so that the queued requests
+				// are finished under the same budget (a running pass always
+				// ends and wakes the waiting workers)
+				const uint64_t free_b = slot.budget > slot.in_flight ? slot.budget - slot.in_flight : 0;
+				return s->pending.front()->est_bytes <= free_b || slot.in_flight == 0;
 			});
 			if (s->pending.empty())
 				return; // stopping, nothing queued
-			uint64_t free_b = s->budget > s->in_flight_bytes ? s->budget - s->in_flight_bytes : 0;
+			const uint64_t free_b = slot.budget > slot.in_flight ? slot.budget - slot.in_flight : 0;
 			// admission in arrival order: the head always (it fits, or runs
-			// alone on an idle device), then followers while they fit
+			// alone on an idle slot), then followers of the same variant while
+			// they fit
 			auto head = s->pending.front();
-			direct = (head->flags & NUCLEUS34_REQ_CLIQUES) != 0;
+			direct = head->direct;
 			batch.push_back(head);
 			s->pending.pop_front();
 			take_bytes = head->est_bytes;
-			uint64_t tri_bound = head->est_triangles;
-			if (!direct)
+			uint64_t tri_bound = head->est_triangles, clique_bound = head->est_cliques;
+			while (!s->pending.empty() && batch.size() < s->max_batch)
 			{
-				while (!s->pending.empty() && batch.size() < s->max_batch)
-				{
-					auto &q = s->pending.front();
-					if (q->flags & NUCLEUS34_REQ_CLIQUES)
-						break;
-					if (take_bytes + q->est_bytes > free_b || tri_bound + q->est_triangles > range_limit)
-						break;
-					take_bytes += q->est_bytes;
-					tri_bound += q->est_triangles;
-					batch.push_back(q);
-					s->pending.pop_front();
-				}
+				auto &q = s->pending.front();
+				if (q->direct != direct)
+					break;
+				if (take_bytes + q->est_bytes > free_b || tri_bound + q->est_triangles > range_limit ||
+					(direct && clique_bound + q->est_cliques > clique_limit))
+					break;
+				take_bytes += q->est_bytes;
+				tri_bound += q->est_triangles;
+				clique_bound += q->est_cliques;
+				batch.push_back(q);
+				s->pending.pop_front();
 			}
-			s->in_flight_bytes += take_bytes;
+			slot.in_flight += take_bytes;
 			s->busy_workers++;
 			const auto now = clk::now();
 			for (auto &q : batch)
 				q->t_start = now;
 		}
-		if (direct)
-			serve_direct(c, *batch[0]);
-		else
-			serve_union(c, batch);
+		serve_union(c, batch, direct);
 		{
 			std::lock_guard<std::mutex> lk(s->mu);
-			s->in_flight_bytes -= take_bytes;
+			slot.in_flight -= take_bytes;
 			s->busy_workers--;
 			s->passes++;
+			if (direct)
+				s->direct_served += batch.size();
 			const auto now = clk::now();
 			for (auto &q : batch)
 			{
@@ -289,18 +309,40 @@ int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_o
 		return fail(NUCLEUS34_E_INVALID, "null argument");
 	*out = nullptr;
 	clear_error();
+	if (sopts && sopts->device_count && !sopts->devices)
+		return fail(NUCLEUS34_E_INVALID, "device_count without devices");
+	if (sopts && sopts->route > NUCLEUS34_ROUTE_ONDEMAND)
+		return fail(NUCLEUS34_E_INVALID, "unknown route");
 	auto *s = new (std::nothrow) nucleus34_server_s();
 	if (!s)
 		return fail(NUCLEUS34_E_OOM_BUDGET, "host allocation failed");
 	if (opts)
 		s->opts = *opts;
 	s->opts.tune_table = nullptr; // read by each worker context as it is created; not kept
-	const uint32_t nw = (sopts && sopts->workers) ? sopts->workers : 2u;
+	const uint32_t per_dev = (sopts && sopts->workers) ? sopts->workers : 2u;
 	s->max_batch = (sopts && sopts->max_batch_graphs) ? sopts->max_batch_graphs : 256;
-	for (uint32_t i = 0; i < nw; ++i)
+	s->route = sopts ? sopts->route : NUCLEUS34_ROUTE_MEMORY;
+	s->direct_div = (sopts && sopts->direct_div) ? sopts->direct_div : DEFAULT_DIRECT_DIV;
+	std::vector<int> devs;
+	if (sopts && sopts->device_count)
+		devs.assign(sopts->devices, sopts->devices + sopts->device_count);
+	else
+		devs.push_back(opts ? opts->device : 0);
+	for (size_t d = 0; d < devs.size(); ++d)
 	{
+		Slot sl;
+		sl.device = devs[d];
+		s->slots.push_back(sl);
+	}
+	// workers: per_dev on every slot, interleaved (worker w on slot w % slots)
+	const size_t nw = size_t(per_dev) * devs.size();
+	for (size_t w = 0; w < nw; ++w)
+	{
+		nucleus34_opts o = opts ? *opts : nucleus34_opts{};
+		const size_t si = w % devs.size();
+		o.device = devs[si];
 		nucleus34_ctx ctx = nullptr;
-		int rc = create_ctx(opts, &ctx);
+		int rc = create_ctx(&o, &ctx);
 		if (rc)
 		{
 			for (auto x : s->ctxs)
@@ -309,13 +351,15 @@ int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_o
 			return rc;
 		}
 		s->ctxs.push_back(ctx);
+		s->worker_slot.push_back(si);
+		// one budget per slot, shared by the passes in flight there
+		if (w < devs.size())
+			s->slots[si].budget = ctx->c.budget;
 	}
-	// one budget shared by the passes in flight
-	s->budget = s->ctxs[0]->c.budget;
-	for (auto x : s->ctxs)
-		x->c.budget = s->budget;
-	for (uint32_t i = 0; i < nw; ++i)
-		s->workers.emplace_back(worker_loop, s, size_t(i));
+	for (size_t w = 0; w < nw; ++w)
+		s->ctxs[w]->c.budget = s->slots[s->worker_slot[w]].budget;
+	for (size_t w = 0; w < nw; ++w)
+		s->workers.emplace_back(worker_loop, s, w);
 	*out = s;
 	return NUCLEUS34_OK;
 }
@@ -343,10 +387,22 @@ int nucleus34_server_submit(nucleus34_server s, const nucleus34_csr *csr, uint32
 	if (acc != csr->m)
 		return fail(NUCLEUS34_E_INVALID, "sum of D does not equal m");
 	q->O[csr->n] = uint32_t(acc);
-	const uint64_t w = wedge_bound(csr->D, csr->n);
+	uint64_t w = 0, t3 = 0;
+	out_bounds(csr->D, csr->n, w, t3);
 	q->est_triangles = w;
-	q->est_bytes = PASS_BYTES_PER_EDGE * csr->m +
-				   (flags & NUCLEUS34_REQ_CLIQUES ? DIRECT_BYTES_PER_WEDGE : PASS_BYTES_PER_TRIANGLE) * w;
+	q->est_cliques = t3;
+	const uint64_t est_on = PASS_BYTES_PER_EDGE * csr->m + PASS_BYTES_PER_TRIANGLE * w;
+	const unsigned __int128 est_dir128 = (unsigned __int128)est_on + (unsigned __int128)DIRECT_BYTES_PER_CLIQUE * t3;
+	const uint64_t est_dir = est_dir128 > ~uint64_t(0) ? ~uint64_t(0) : uint64_t(est_dir128);
+	// routing by the memory estimate (the smallest slot budget is the limit)
+	uint64_t min_budget = ~uint64_t(0);
+	for (auto &sl : s->slots)
+		min_budget = std::min(min_budget, sl.budget);
+	if (flags & NUCLEUS34_REQ_CLIQUES)
+		q->direct = true;
+	else if (s->route == NUCLEUS34_ROUTE_MEMORY)
+		q->direct = est_dir <= min_budget / s->direct_div && t3 < 0xffffffffull;
+	q->est_bytes = q->direct ? est_dir : est_on;
 	q->t_submit = clk::now();
 	{
 		std::lock_guard<std::mutex> lk(s->mu);
@@ -381,7 +437,7 @@ int nucleus34_server_wait(nucleus34_server s, uint64_t id, int64_t timeout_ms, n
 		x.queue_seconds = std::chrono::duration<double>(q->t_start - q->t_submit).count();
 		x.latency_seconds = std::chrono::duration<double>(q->t_done - q->t_submit).count();
 		x.pass = q->pass;
-		x.direct = (q->flags & NUCLEUS34_REQ_CLIQUES) ? 1 : 0;
+		x.direct = q->direct ? 1 : 0;
 		*info = x;
 	}
 	if (q->status)
@@ -450,8 +506,13 @@ int nucleus34_server_stats(nucleus34_server s, nucleus34_server_counters *out)
 	x.pending = s->pending.size();
 	x.busy_workers = s->busy_workers;
 	x.workers = s->workers.size();
-	x.in_flight_bytes = s->in_flight_bytes;
-	x.budget_bytes = s->budget;
+	for (auto &sl : s->slots)
+	{
+		x.in_flight_bytes += sl.in_flight;
+		x.budget_bytes += sl.budget;
+	}
+	x.direct_served = s->direct_served;
+	x.devices = s->slots.size();
 	*out = x;
 	return NUCLEUS34_OK;
 }

@@ -57,6 +57,7 @@ EXPORTED = (
     "nucleus34_graph_release", "nucleus34_graph_csr",
     "nucleus34_gen_rmat", "nucleus34_gen_rgg", "nucleus34_gen_ws",
     "nucleus34_edges_write", "nucleus34_edges_release", "nucleus34_splitmix64",
+    "nucleus34_graph_cost", "nucleus34_split_plan",
 )
 
 
@@ -133,7 +134,8 @@ class GraphSummary(C.Structure):
 
 
 class ServerOpts(C.Structure):
-    _fields_ = [("workers", C.c_uint32), ("max_batch_graphs", C.c_uint64)]
+    _fields_ = [("workers", C.c_uint32), ("max_batch_graphs", C.c_uint64), ("route", C.c_uint32),
+                ("direct_div", C.c_uint32), ("device_count", C.c_uint32), ("devices", C.POINTER(C.c_int))]
 
 
 class RequestInfo(C.Structure):
@@ -147,7 +149,7 @@ class RequestInfo(C.Structure):
 
 class ServerCounters(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("passes", "served", "pending", "busy_workers", "workers",
-                                          "in_flight_bytes", "budget_bytes")]
+                                          "in_flight_bytes", "budget_bytes", "direct_served", "devices")]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -203,6 +205,11 @@ def lib() -> C.CDLL:
     L.nucleus34_batch_copy_k.restype = C.c_int
     L.nucleus34_batch_free.argtypes = [C.c_void_p]
     L.nucleus34_batch_free.restype = None
+    L.nucleus34_graph_cost.argtypes = [C.POINTER(Csr), C.POINTER(C.c_uint64)]
+    L.nucleus34_graph_cost.restype = C.c_int
+    L.nucleus34_split_plan.argtypes = [C.POINTER(C.c_uint64), C.c_uint64, C.c_uint32, C.POINTER(C.c_uint32),
+                                       C.POINTER(C.c_uint64)]
+    L.nucleus34_split_plan.restype = C.c_int
     L.nucleus34_server_create.argtypes = [C.POINTER(Opts), C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]
     L.nucleus34_server_create.restype = C.c_int
     L.nucleus34_server_submit.argtypes = [C.c_void_p, C.POINTER(Csr), C.c_uint32, C.POINTER(C.c_uint64)]
@@ -294,6 +301,27 @@ def splitmix64(x: int) -> int:
 
 
 # ---------------------------------------------------------------- graphs ----
+
+def graph_cost(g: "HostGraph") -> int:
+    """Estimated cost of decomposing g: oriented edges plus out-wedges."""
+    c = C.c_uint64()
+    csr = g.csr()
+    _check(lib().nucleus34_graph_cost(C.byref(csr), C.byref(c)), "graph_cost")
+    return int(c.value)
+
+
+def split_plan(costs, parts: int):
+    """Share of each graph when `len(costs)` graphs are split over `parts`
+    replicas (nucleus34_split_plan: greedy longest-processing-time,
+    deterministic). Returns (part_of, load) as numpy arrays."""
+    c = np.ascontiguousarray(np.asarray(costs, dtype=np.uint64))
+    part_of = np.zeros(len(c), np.uint32)
+    load = np.zeros(max(parts, 1), np.uint64)
+    _check(lib().nucleus34_split_plan(c.ctypes.data_as(C.POINTER(C.c_uint64)), len(c), parts,
+                                      _u32p(part_of) if len(c) else None,
+                                      load.ctypes.data_as(C.POINTER(C.c_uint64))), "split_plan")
+    return part_of, load[:parts]
+
 
 @dataclass
 class HostGraph:
@@ -501,16 +529,93 @@ def batch_decompose(graphs, device: int = 0, mem_budget_bytes: int = 0, flags: i
 
 REQ_CLIQUES = 0x1
 REQ_TRIANGLES = 0x2
+ROUTE_MEMORY = 0
+ROUTE_ONDEMAND = 1
+
+
+class DeviceBatch:
+    """Graphs split over several devices (replicas, no collective): each
+    device decomposes its share as one nucleus34_batch_decompose, all shares
+    at once on host threads (the C calls release the GIL). Results are read
+    by global graph index, like a Batch."""
+
+    def __init__(self, parts, where, result):
+        self._parts, self._where, self.result = parts, where, result
+
+    def summary(self, i: int) -> dict:
+        p, j = self._where[i]
+        return self._parts[p].summary(j)
+
+    def copy_k(self, i: int, with_tris: bool = False):
+        p, j = self._where[i]
+        return self._parts[p].copy_k(j, with_tris)
+
+    def close(self) -> None:
+        for b in self._parts:
+            if b is not None:
+                b.close()
+        self._parts = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def batch_decompose_devices(graphs, devices, mem_budget_bytes: int = 0, flags: int = 0) -> DeviceBatch:
+    """The batched form over several devices: nucleus34_split_plan assigns
+    each graph to one device by estimated cost, every device runs its share
+    as a batch, and results stay addressed by the caller's graph index. A
+    device may appear more than once (several shares on one GPU)."""
+    import threading
+    devices = list(devices)
+    part_of, load = split_plan([graph_cost(g) for g in graphs], len(devices))
+    shares = [[i for i in range(len(graphs)) if part_of[i] == p] for p in range(len(devices))]
+    parts = [None] * len(devices)
+    errors = [None] * len(devices)
+
+    def run(p):
+        try:
+            if shares[p]:
+                parts[p] = batch_decompose([graphs[i] for i in shares[p]], device=devices[p],
+                                           mem_budget_bytes=mem_budget_bytes, flags=flags)
+        except BaseException as e:  # reported below, after every share has ended
+            errors[p] = e
+
+    threads = [threading.Thread(target=run, args=(p,)) for p in range(len(devices))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    for e in errors:
+        if e is not None:
+            for b in parts:
+                if b is not None:
+                    b.close()
+            raise e
+    where = {}
+    for p, idx in enumerate(shares):
+        for j, i in enumerate(idx):
+            where[i] = (p, j)
+    res = {"devices": devices, "share_graphs": [len(x) for x in shares], "share_cost": [int(x) for x in load],
+           "shares": [b.result if b is not None else None for b in parts]}
+    return DeviceBatch(parts, where, res)
 
 
 class Server:
     """nucleus34_server_*: continuous batching of decomposition requests."""
 
     def __init__(self, device: int = 0, mem_budget_bytes: int = 0, workers: int = 2, max_batch_graphs: int = 256,
-                 flags: int = 0):
+                 flags: int = 0, route: int = ROUTE_MEMORY, direct_div: int = 0, devices=None):
+        """workers: concurrent passes per device slot; devices: slot ordinals
+        (one may repeat), mem_budget_bytes applies to each slot; route and
+        direct_div: the variant chosen per request by its memory estimate."""
         self._L = lib()
         opts = make_opts(device, mem_budget_bytes, flags=flags)
-        so = ServerOpts(workers, max_batch_graphs)
+        self._devs = (C.c_int * len(devices))(*devices) if devices else None
+        so = ServerOpts(workers, max_batch_graphs, route, direct_div, len(devices) if devices else 0,
+                        C.cast(self._devs, C.POINTER(C.c_int)) if devices else None)
         self._h = C.c_void_p()
         _check(self._L.nucleus34_server_create(C.byref(opts), C.byref(so), C.byref(self._h)), "server_create")
 

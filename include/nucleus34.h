@@ -317,26 +317,54 @@ int nucleus34_batch_summary(nucleus34_batch b, uint64_t index, nucleus34_graph_s
 int nucleus34_batch_copy_k(nucleus34_batch b, uint64_t index, int32_t *k_out, uint32_t *tris_out);
 void nucleus34_batch_free(nucleus34_batch b);
 
+/* ---- replicas over several GPUs: the split of independent graphs ---------- */
+
+/* No reference counterpart (the reference runs one graph per process). A
+ * graph's estimated cost: its oriented edges plus its out-wedges
+ * sum_u d+(u)(d+(u)-1)/2 (the admission estimates' bound on its triangles). */
+int nucleus34_graph_cost(const nucleus34_csr *g, uint64_t *cost);
+/* Partitions `count` graphs of the given costs into `parts` shares
+ * (part_of[i] in [0, parts)) by the greedy longest-processing-time rule:
+ * decreasing cost, ties by index, each to the least-loaded share (ties by
+ * share number). Deterministic, so every rank derives the same plan. load
+ * (optional, parts entries) receives each share's total cost. */
+int nucleus34_split_plan(const uint64_t *cost, uint64_t count, uint32_t parts, uint32_t *part_of, uint64_t *load);
+
 /* ---- serving: continuous batching of decomposition requests -------------- */
 
 /* A request loop with device-resident state. Workers (one context and stream
- * each) admit pending requests in arrival order while their estimated memory
- * fits what the budget (opts.mem_budget_bytes) has left, decompose them in one
- * union pass, and copy each request's results to the host. Requests that
- * arrive while passes run join the next pass; passes of different workers
- * overlap on the device. Requests flagged NUCLEUS34_REQ_CLIQUES are routed to
- * the direct variant (their four-clique list is kept) and run alone; all
- * others run on-demand. A request's results equal those of the graph
- * decomposed alone. No reference counterpart. */
+ * each, spread over one or more devices) admit pending requests in arrival
+ * order while their estimated memory fits what their device's budget
+ * (opts.mem_budget_bytes per device) has left, decompose them in one union
+ * pass, and copy each request's results to the host. Requests that arrive
+ * while passes run join the next pass; passes of different workers overlap
+ * on the device. Each request's variant is chosen at submission by its
+ * memory estimate (bytes per oriented edge and per out-wedge, plus, for the
+ * direct variant, per out-triple sum_u C(d+(u), 3), the bound on its
+ * four-cliques that the clique list grows with): with NUCLEUS34_ROUTE_MEMORY
+ * it is the direct variant when that estimate is at most 1/direct_div of a
+ * device's budget, else on-demand; requests flagged NUCLEUS34_REQ_CLIQUES are
+ * always direct. A pass holds requests of one variant; direct unions stay
+ * below 2^32 four-cliques by the same bound. A request's results equal those
+ * of the graph decomposed alone. No reference counterpart: the reference's
+ * projection of the direct peel's memory (cuNucleus34.cu:563-585) only
+ * reports whether that peel will fit. */
 typedef struct nucleus34_server_s *nucleus34_server;
 
 #define NUCLEUS34_REQ_CLIQUES 0x1u   /* direct variant: keep the four-clique list */
 #define NUCLEUS34_REQ_TRIANGLES 0x2u /* keep the triangle list (k alone otherwise) */
 
+#define NUCLEUS34_ROUTE_MEMORY 0u    /* direct when its estimate fits 1/direct_div of a device's budget */
+#define NUCLEUS34_ROUTE_ONDEMAND 1u  /* on-demand unless the request asks for its clique list */
+
 typedef struct
 {
-	uint32_t workers;             /* concurrent passes, 0 = 2 */
+	uint32_t workers;             /* concurrent passes per device, 0 = 2 */
 	uint64_t max_batch_graphs;    /* requests per pass, 0 = 256 */
+	uint32_t route;               /* NUCLEUS34_ROUTE_* */
+	uint32_t direct_div;          /* ROUTE_MEMORY: direct estimate <= budget / direct_div; 0 = default */
+	uint32_t device_count;        /* 0: opts.device alone; else devices[0..device_count) */
+	const int *devices;           /* ordinals (one may repeat: several budgets on one GPU) */
 } nucleus34_server_opts;
 
 typedef struct
@@ -352,6 +380,8 @@ typedef struct
 typedef struct
 {
 	uint64_t passes, served, pending, busy_workers, workers, in_flight_bytes, budget_bytes;
+	uint64_t direct_served;       /* requests served by the direct variant */
+	uint64_t devices;             /* device slots */
 } nucleus34_server_counters;
 
 int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_opts *sopts, nucleus34_server *out);

@@ -109,3 +109,19 @@ def test_batch_results_moved_to_host_are_unchanged(n34):
             assert np.array_equal(kd, kh) and np.array_equal(td, th)
             assert np.array_equal(kh, single[i].k)
             assert host.summary(i) == dev.summary(i)
+
+
+@pytest.mark.gpu
+def test_batch_split_over_device_shares_equals_one_batch(n34):
+    """The batched form over several device shares (nucleus34_split_plan,
+    here two shares on GPU 0 running at once): every graph's summary, k and
+    triangles equal the single batch's."""
+    graphs = _mixed_graphs(n34, 32, 13)
+    with n34.batch_decompose(graphs) as one, n34.batch_decompose_devices(graphs, [0, 0]) as two:
+        assert sorted(two.result["share_graphs"]) == sorted(two.result["share_graphs"]) and \
+            sum(two.result["share_graphs"]) == len(graphs) and min(two.result["share_graphs"]) > 0
+        for i in range(len(graphs)):
+            k1, t1 = one.copy_k(i, with_tris=True)
+            k2, t2 = two.copy_k(i, with_tris=True)
+            assert np.array_equal(k1, k2) and np.array_equal(t1, t2)
+            assert one.summary(i) == two.summary(i)
