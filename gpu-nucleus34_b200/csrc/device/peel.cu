@@ -27,6 +27,7 @@
 // stamps, and crossing detection catches every triangle that reaches the level.
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "intersect.cuh"
@@ -61,6 +62,8 @@ struct CtlX
 	uint32_t compactions;
 	unsigned long long t0_ns; // %globaltimer at the peel's start (device-loop time bound)
 	uint32_t timed_out;       // the device loop stopped at its round or time bound
+	uint32_t small_rounds;    // rounds run inside k_small_rounds
+	uint32_t loop_passes;     // passes of the device loop's body
 	// profiling counters of k_debit_flags_warp (filled only when stats is set)
 	uint32_t stats;
 	unsigned long long st_tri, st_merge_entries, st_steps, st_lookups, st_resolves, st_staged, st_found;
@@ -148,6 +151,8 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl, uint
 		asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
 		ctl->t0_ns = now;
 		ctl->timed_out = 0;
+		ctl->small_rounds = 0;
+		ctl->loop_passes = 0;
 		ctl->compactions = 0;
 		ctl->st_tri = ctl->st_merge_entries = ctl->st_steps = ctl->st_lookups = 0;
 		ctl->st_resolves = ctl->st_staged = ctl->st_found = 0;
@@ -1524,6 +1529,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, 4) k_small_rounds(
 			c.nNext = 0;
 			c.minS = INF;
 			ctl->scan = nNext == 0;
+			ctl->small_rounds++;
 #if N34_DEBIT_CURSOR
 			ctl->cursor = 0;
 #endif
@@ -1548,6 +1554,7 @@ __global__ void k_loop_cond(CtlX *ctl, cudaGraphConditionalHandle h, uint32_t ma
 {
 	unsigned long long now;
 	asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+	ctl->loop_passes++;
 	bool more = !ctl->c.done && !ctl->c.error;
 	if (more && (ctl->c.round > max_rounds || now - ctl->t0_ns > limit_ns))
 	{
@@ -1953,6 +1960,9 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			CtlX hx{};
 			if (!rc && cudaMemcpy(&hx, ctl, sizeof(CtlX), cudaMemcpyDeviceToHost) != cudaSuccess)
 				rc = fail(NUCLEUS34_E_CUDA, "peel control");
+			if (!rc && std::getenv("NUCLEUS34_PEEL_VERBOSE"))
+				std::fprintf(stderr, "[peel] rounds=%u peeling_rounds=%u small_rounds=%u loop_passes=%u compactions=%u\n",
+							 hx.c.round, hx.c.rounds, hx.small_rounds, hx.loop_passes, hx.compactions);
 			if (!rc)
 			{
 				rounds = hx.c.round;
