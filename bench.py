@@ -61,7 +61,7 @@ def parse():
     p.add_argument("--cpu-sample-scale", type=int, default=14)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="decompose", choices=["decompose", "batch", "serve"],
+    p.add_argument("--workload", default="decompose", choices=["decompose", "batch", "serve", "variants"],
                    help="decompose: the headline single-graph metric; batch: the batched form "
                         "(graphs/s of nucleus34_batch_decompose vs one decomposition per graph)")
     p.add_argument("--capture-run", action="store_true",
@@ -516,6 +516,41 @@ def run_serve(a):
     return 0 if mism == 0 else 1
 
 
+def run_variants(a):
+    """Direct against on-demand by graph size: device time (median of 3 warm
+    runs on one context) and measured peak bytes of both variants on seeded
+    graphs of serving sizes, one JSON line per graph (the data behind the
+    serving loop's routing rule)."""
+    import numpy as np
+    import nucleus34 as n34
+    cases = [("rmat", s, ef, 7) for s in (8, 10, 12, 14, 16) for ef in (8, 16, 24)] + \
+            [("rgg", n, d, 3) for n in (2000, 20000, 200000) for d in (16.0, 32.0, 64.0)] + \
+            [("ws", n, 10, 5) for n in (1000, 10000, 100000)]
+    for kind, x, y, seed in cases:
+        if kind == "rmat":
+            s, d = n34.gen_rmat(x, y, seed)
+        elif kind == "rgg":
+            s, d = n34.gen_rgg(x, y, seed)
+        else:
+            s, d = n34.gen_ws(x, y, 0.1, seed)
+        g = n34.graph_from_edges(s, d)
+        D = g.D.astype(np.int64)
+        row = {"graph": f"{kind} {x} {y}", "n": g.n, "m": g.m, "wedges": int((D * (D - 1) // 2).sum()),
+               "triples": int((D * (D - 1) * (D - 2) // 6).sum())}
+        with n34.Context() as ctx:
+            ctx.upload(g)
+            for v in ("ondemand", "direct"):
+                ctx.run(v)
+                ts = []
+                for _ in range(3):
+                    r = ctx.run(v)
+                    ts.append(r["t_total"])
+                row[v] = {"t_ms": 1e3 * float(np.median(ts)), "peak": int(r["peak_device_bytes"]),
+                          "T": int(r["triangle_count"]), "Q": int(r["four_clique_count"])}
+        print(json.dumps(row), flush=True)
+    return 0
+
+
 def capture_run(a):
     """One decomposition and nothing else, so that ncu launch indices are
     those of that decomposition alone."""
@@ -559,6 +594,8 @@ def main():
         return run_batch(a)
     if a.workload == "serve":
         return run_serve(a)
+    if a.workload == "variants":
+        return run_variants(a)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
     local = int(os.environ.get("LOCAL_RANK", "0"))
