@@ -116,12 +116,31 @@ int Ctx::alloc(void **p, uint64_t bytes, const char *what)
 	if (bytes == 0)
 		bytes = 16;
 	bytes = (bytes + 255) & ~uint64_t(255);
+	auto hit = kept.find(bytes);
+	if (hit != kept.end())
+	{
+		*p = hit->second;
+		kept.erase(hit);
+		kept_bytes -= bytes;
+		in_use += bytes;
+		peak = std::max(peak, in_use);
+		sizes[*p] = bytes;
+		return NUCLEUS34_OK;
+	}
+	if (in_use + kept_bytes + bytes > budget)
+		trim_kept();
 	if (in_use + bytes > budget)
 		return fail(NUCLEUS34_E_OOM_BUDGET, std::string("device memory budget exceeded allocating ") + what + " (" +
 												std::to_string(bytes >> 20) + " MiB; in use " +
 												std::to_string(in_use >> 20) + " of " + std::to_string(budget >> 20) +
 												" MiB)");
 	cudaError_t e = cudaMallocAsync(p, bytes, stream);
+	if (e == cudaErrorMemoryAllocation && kept_bytes)
+	{
+		cudaGetLastError();
+		trim_kept();
+		e = cudaMallocAsync(p, bytes, stream);
+	}
 	if (e != cudaSuccess)
 	{
 		cudaGetLastError();
@@ -143,9 +162,24 @@ void Ctx::release(void *p)
 	if (it != sizes.end())
 	{
 		in_use -= it->second;
+		if (keep_blocks)
+		{
+			kept.emplace(it->second, p);
+			kept_bytes += it->second;
+			sizes.erase(it);
+			return;
+		}
 		sizes.erase(it);
 	}
 	cudaFreeAsync(p, stream);
+}
+
+void Ctx::trim_kept()
+{
+	for (auto &kv : kept)
+		cudaFreeAsync(kv.second, stream);
+	kept.clear();
+	kept_bytes = 0;
 }
 
 void Ctx::release_results()
@@ -697,6 +731,8 @@ void destroy_ctx(nucleus34_ctx x)
 	cudaSetDevice(c.device);
 	c.release_results();
 	c.release_graph();
+	c.trim_kept();
+	c.keep_blocks = false;
 	for (auto &kv : c.sizes)
 		cudaFreeAsync(kv.first, c.stream);
 	c.sizes.clear();
@@ -773,7 +809,13 @@ int nucleus34_ctx_create(const nucleus34_opts *opts, nucleus34_ctx *out)
 {
 	if (!out)
 		return fail(NUCLEUS34_E_INVALID, "null output");
-	return guarded([&] { return create_ctx(opts, out); });
+	return guarded([&] {
+		const int rc = create_ctx(opts, out);
+		// a resident context usually runs again: it keeps its blocks
+		if (!rc)
+			(*out)->c.keep_blocks = true;
+		return rc;
+	});
 }
 
 int nucleus34_ctx_upload(nucleus34_ctx ctx, const nucleus34_csr *csr)

@@ -135,9 +135,18 @@ struct Ctx
 	uint64_t *dseg = nullptr; // device: eoff (count+1), toff (count+1), q, ksum (count), kmax (count, u32 words)
 
 	std::unordered_map<void *, uint64_t> sizes; // live allocations
+	// Released blocks kept for reuse by a later allocation of the same size
+	// on this context's stream (contexts that run the same graph again: every
+	// run then finds its blocks, and the device pool never has to grow in
+	// the middle of a phase). Off unless keep_blocks; trimmed when the budget
+	// or the device needs the memory, and when the context is destroyed.
+	bool keep_blocks = false;
+	std::unordered_multimap<uint64_t, void *> kept;
+	uint64_t kept_bytes = 0;
 
 	int alloc(void **p, uint64_t bytes, const char *what);
 	void release(void *p);
+	void trim_kept();
 	void release_results();
 	void release_graph();
 };

@@ -1468,32 +1468,22 @@ __global__ void __launch_bounds__(PEEL_THREADS, 4) k_small_rounds(
 			aborted = true;
 			break;
 		}
-		// debit: a warp takes 32 frontier entries; short ones a lane each,
-		// then the long ones one after the other with the whole warp
-		for (uint64_t base = warp * 32; base < nF; base += nwarps * 32)
+		// debit: triangles whose shortest list is short one thread each, then
+		// the others one warp each (the split of the regular kernels; both
+		// passes only append to the next frontier, so no barrier between)
+		for (uint64_t i = tid; i < nF; i += nthreads)
 		{
-			const uint64_t i = base + lane;
-			const bool have = i < nF;
-			uint32_t t = 0;
-			Lists L{0, 0, 0, 0, 0, 0};
-			if (have)
-			{
-				t = __ldcg(F + i);
-				L = frontier_lists(t, tris, span);
-			}
-			const bool is_long = have && (L.a1 - L.a0 > LANE_MAX);
-			if (have && !is_long)
+			const uint32_t t = __ldcg(F + i);
+			const Lists L = frontier_lists(t, tris, span);
+			if (L.a1 - L.a0 <= LANE_MAX)
 				debit_thread_tri<LANE_MAX, false, true>(t, L, ctl, Fn, nullptr, third, itri, S, level, T);
-			uint32_t longs = __ballot_sync(FULL, is_long);
-			while (longs)
-			{
-				const uint32_t sl = __ffs(longs) - 1;
-				longs &= longs - 1;
-				const uint32_t tt = __shfl_sync(FULL, t, sl);
-				const Lists LL{__shfl_sync(FULL, L.a0, sl), __shfl_sync(FULL, L.a1, sl), __shfl_sync(FULL, L.b0, sl),
-							   __shfl_sync(FULL, L.b1, sl), __shfl_sync(FULL, L.c0, sl), __shfl_sync(FULL, L.c1, sl)};
-				debit_warp_tri<false, true>(tt, LL, sm, ctl, Fn, nullptr, third, itri, S, level, T);
-			}
+		}
+		for (uint64_t i = warp; i < nF; i += nwarps)
+		{
+			const uint32_t t = __ldcg(F + i);
+			const Lists L = frontier_lists(t, tris, span);
+			if (L.a1 - L.a0 > LANE_MAX) // warp-uniform
+				debit_warp_tri<false, true>(t, L, sm, ctl, Fn, nullptr, third, itri, S, level, T);
 		}
 		if (!grid_barrier(bar, gen, deadline))
 		{

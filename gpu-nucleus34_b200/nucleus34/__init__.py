@@ -421,8 +421,16 @@ OPT_HOST_LOOP = 0x20
 OPT_NO_SMALL_ROUNDS = 0x40
 
 
+# The tune table the autotuner wrote on a B200 for this build's measured graph
+# classes; used when no other table is given ("" selects the built-in
+# defaults).
+SHIPPED_TUNE_TABLE = os.path.join(ROOT_DIR, "tune", "b200.tune")
+
+
 def make_opts(device: int = 0, mem_budget_bytes: int = 0, parts: int = 1, flags: int = 0,
               tune_table: Optional[str] = None) -> Opts:
+    if tune_table is None and os.path.exists(SHIPPED_TUNE_TABLE):
+        tune_table = SHIPPED_TUNE_TABLE
     return Opts(mem_budget_bytes, device, parts, os.fsencode(tune_table) if tune_table else None, flags)
 
 

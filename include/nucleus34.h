@@ -184,6 +184,10 @@ const char *nucleus34_last_error(void);
 
 typedef struct nucleus34_ctx_s *nucleus34_ctx;
 
+/* A context keeps the device blocks its runs release and reuses them for
+ * allocations of the same size, so a graph run again allocates nothing new;
+ * the kept blocks count toward opts.mem_budget_bytes, are given back when an
+ * allocation needs the room, and are freed by nucleus34_ctx_destroy. */
 int nucleus34_ctx_create(const nucleus34_opts *opts, nucleus34_ctx *out);
 /* H2D copy of the CSR into context-owned device memory (replaces the
  * thrust::device_vector uploads, cuNucleus34.cu:290-293). */
