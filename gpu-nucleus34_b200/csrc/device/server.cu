@@ -5,7 +5,9 @@
 // slot; a slot is a device with its own memory budget, and several slots may
 // name one GPU. A worker takes the pending requests in arrival order that fit
 // the memory still free in its slot (estimated per request from its CSR) and
-// within the 32-bit ranges, decomposes them in one pass as a disjoint union
+// within the 32-bit ranges (same-variant requests further back in the queue
+// join too, past requests of the other variant), decomposes them in one pass
+// as a disjoint union
 // (the batched form), copies every request's results to the host and signals
 // it. Requests that arrive while passes run are admitted by the next free
 // worker, so with two or more workers their passes overlap on the device.
@@ -239,27 +241,32 @@ void worker_loop(nucleus34_server_s *s, size_t wi)
 				return; // stopping, nothing queued
 			const uint64_t free_b = slot.budget > slot.in_flight ? slot.budget - slot.in_flight : 0;
 			// admission in arrival order: the head always (it fits, or runs
-			// alone on an idle slot), then followers of the same variant while
-			// they fit
+			// alone on an idle slot), then, in order, the pending requests of
+			// the same variant that fit, looking past requests of the other
+			// variant (they stay queued for the next pass) within a bounded
+			// window, so that interleaved variants still fill their passes
 			auto head = s->pending.front();
 			direct = head->direct;
 			batch.push_back(head);
 			s->pending.pop_front();
 			take_bytes = head->est_bytes;
 			uint64_t tri_bound = head->est_triangles, clique_bound = head->est_cliques;
-			while (!s->pending.empty() && batch.size() < s->max_batch)
+			const size_t window = 4 * s->max_batch;
+			for (size_t i = 0; i < s->pending.size() && i < window && batch.size() < s->max_batch;)
 			{
-				auto &q = s->pending.front();
-				if (q->direct != direct)
-					break;
-				if (take_bytes + q->est_bytes > free_b || tri_bound + q->est_triangles > range_limit ||
+				auto &q = s->pending[i];
+				if (q->direct != direct || take_bytes + q->est_bytes > free_b ||
+					tri_bound + q->est_triangles > range_limit ||
 					(direct && clique_bound + q->est_cliques > clique_limit))
-					break;
+				{
+					++i;
+					continue;
+				}
 				take_bytes += q->est_bytes;
 				tri_bound += q->est_triangles;
 				clique_bound += q->est_cliques;
 				batch.push_back(q);
-				s->pending.pop_front();
+				s->pending.erase(s->pending.begin() + std::ptrdiff_t(i));
 			}
 			slot.in_flight += take_bytes;
 			s->busy_workers++;
