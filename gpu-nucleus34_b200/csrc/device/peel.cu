@@ -1078,8 +1078,14 @@ __device__ __forceinline__ bool sort_wanted(const CtlX *ctl, uint64_t T)
 	return !ctl->c.done && ctl->c.nNext >= ctl->sort_min && ctl->c.nNext <= T;
 }
 
+// Sort key of a frontier triangle: its id, or, with cpos (the entry
+// positions of the triangles' c edges, 3t + 2 of tpos), the position of its
+// entry under c. Entry positions are edge-major, so the second order groups
+// the triangles that share their c edge (v -> w, between the two vertices of
+// higher degree: usually their longest list, the one every lookup searches).
 __global__ void k_fsort_set(const CtlX *ctl, const uint32_t *__restrict__ F0, const uint32_t *__restrict__ F1,
-							uint32_t *__restrict__ bits, uint64_t T)
+							uint32_t *__restrict__ bits, uint64_t T, const uint32_t *__restrict__ tpos,
+							uint64_t keys)
 {
 	if (!sort_wanted(ctl, T))
 		return;
@@ -1089,8 +1095,11 @@ __global__ void k_fsort_set(const CtlX *ctl, const uint32_t *__restrict__ F0, co
 	for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += stride)
 	{
 		const uint32_t t = Fn[i];
-		if (t < T)
-			atomicOr(bits + (t >> 5), 1u << (t & 31));
+		if (t >= T)
+			continue;
+		const uint32_t k = tpos ? tpos[3 * uint64_t(t) + 2] : t;
+		if (k < keys)
+			atomicOr(bits + (k >> 5), 1u << (k & 31));
 	}
 }
 
@@ -1180,7 +1189,7 @@ __global__ void __launch_bounds__(1024) k_fsort_scan(const CtlX *ctl, uint32_t *
 __global__ void __launch_bounds__(SORT_THREADS) k_fsort_write(const CtlX *ctl, uint32_t *__restrict__ bits,
 															   uint64_t W, const uint32_t *__restrict__ chunk,
 															   uint32_t *__restrict__ F0, uint32_t *__restrict__ F1,
-															   uint64_t T)
+															   uint64_t T, const uint32_t *__restrict__ itri)
 {
 	if (!sort_wanted(ctl, T))
 		return;
@@ -1224,7 +1233,11 @@ __global__ void __launch_bounds__(SORT_THREADS) k_fsort_write(const CtlX *ctl, u
 				const uint32_t b = __ffs(m) - 1;
 				m &= m - 1;
 				if (pos < n)
-					Fn[pos] = uint32_t((w0 + k) * 32 + b);
+				{
+					const uint32_t key = uint32_t((w0 + k) * 32 + b);
+					// an entry position names its triangle (flags masked)
+					Fn[pos] = itri ? (itri[key] & ID_MASK) : key;
+				}
 				++pos;
 			}
 			if (wv[k])
@@ -1766,9 +1779,14 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			uint32_t(std::min<unsigned long long>(N34_SMALL_MAX, sort_min > 0 ? sort_min - 1 : 0));
 		// frontier ordering bitmap (optional: skipped without room for it;
 		// a bitmap frontier is in id order already)
-		const uint64_t fchunks = (fwords + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
+		// keyed by the c-edge entry position (3T keys) when asked and the entry
+		// positions exist (death-flag peel), else by triangle id (T keys)
+		const bool order_by_c = flags && inc.tpos && (c.opt_flags & NUCLEUS34_OPT_FRONTIER_BY_C);
+		const uint64_t fkeys = order_by_c ? 3 * T : T;
+		const uint64_t skeys_words = (fkeys + 31) / 32;
+		const uint64_t fchunks = (skeys_words + SORT_CHUNK_WORDS - 1) / SORT_CHUNK_WORDS;
 		if (!sort_on || lean || (c.opt_flags & NUCLEUS34_OPT_LEAN_MEMORY) ||
-			dalloc(c, &fbits, fwords, "frontier order bitmap") ||
+			dalloc(c, &fbits, skeys_words, "frontier order bitmap") ||
 			dalloc(c, &fchunk, fchunks, "frontier order chunks"))
 		{
 			c.release(fbits);
@@ -1777,7 +1795,7 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			fchunk = nullptr;
 			clear_error();
 		}
-		else if (cudaMemsetAsync(fbits, 0, fwords * 4, c.stream) != cudaSuccess)
+		else if (cudaMemsetAsync(fbits, 0, skeys_words * 4, c.stream) != cudaSuccess)
 		{
 			rc = fail(NUCLEUS34_E_CUDA, "memset");
 			break;
@@ -1875,10 +1893,12 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 			}
 			if (fbits)
 			{
-				k_fsort_set<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, fbits, T);
-				k_fsort_count<<<gsort, SORT_THREADS, 0, c.stream>>>(ctl, fbits, fwords, fchunk, T);
+				k_fsort_set<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, F0, F1, fbits, T,
+																  order_by_c ? inc.tpos : nullptr, fkeys);
+				k_fsort_count<<<gsort, SORT_THREADS, 0, c.stream>>>(ctl, fbits, skeys_words, fchunk, T);
 				k_fsort_scan<<<1, 1024, 0, c.stream>>>(ctl, fchunk, fchunks, T);
-				k_fsort_write<<<gsort, SORT_THREADS, 0, c.stream>>>(ctl, fbits, fwords, fchunk, F0, F1, T);
+				k_fsort_write<<<gsort, SORT_THREADS, 0, c.stream>>>(ctl, fbits, skeys_words, fchunk, F0, F1, T,
+																	order_by_c ? inc.tri : nullptr);
 			}
 			k_advance<<<1, 1, 0, c.stream>>>(ctl);
 			if (ev)

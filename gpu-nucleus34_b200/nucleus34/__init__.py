@@ -419,6 +419,7 @@ OPT_VERIFIABLE = 0x8
 OPT_HOST_RESULTS = 0x10
 OPT_HOST_LOOP = 0x20
 OPT_NO_SMALL_ROUNDS = 0x40
+OPT_FRONTIER_BY_C = 0x80
 
 
 # The tune table the autotuner wrote on a B200 for this build's measured graph

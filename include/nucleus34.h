@@ -111,6 +111,11 @@ typedef struct
  * steps of a round (the default for the on-demand peel with death flags).
  * Results are identical; kept for comparison. */
 #define NUCLEUS34_OPT_NO_SMALL_ROUNDS 0x40u
+/* opts.flags: put large peel frontiers in the order of their triangles'
+ * entries under their c edges (edge-major: triangles that share their c edge,
+ * usually their longest list, become neighbours) instead of triangle-id
+ * order. Results are identical. */
+#define NUCLEUS34_OPT_FRONTIER_BY_C 0x80u
 
 typedef struct
 {

@@ -174,3 +174,24 @@ def test_listing_chunks_match_one_pass(n34, oracle):
         r = subprocess.run([sys.executable, "-c", code, pkg], capture_output=True, text=True, timeout=300, env=env)
         assert r.returncode == 0, r.stderr[-2000:]
         assert json.loads(r.stdout.strip().splitlines()[-1]) == want, cap
+
+
+@pytest.mark.parametrize("case", [("rmat", 14, 16, 2), ("rgg", 40000, 48, 6)])
+def test_frontier_ordered_by_c_edge_matches(n34, oracle, case):
+    """Large frontiers put in the order of their c-edge entries (instead of
+    triangle ids) give the oracle's k; the peel's schedule changes, not its
+    result."""
+    if case[0] == "rmat":
+        s, t = n34.gen_rmat(case[1], case[2], case[3])
+    else:
+        s, t = n34.gen_rgg(case[1], case[2], case[3])
+    g = n34.graph_from_edges(s, t)
+    o = oracle.decompose(g)
+    d = n34.decompose(g, variant="ondemand", flags=n34.OPT_FRONTIER_BY_C, n_quds=0)
+    assert np.array_equal(d.k, o.k)
+    # with the sort forced onto every frontier of at least 4096 triangles
+    with n34.Context(flags=n34.OPT_FRONTIER_BY_C) as ctx:
+        ctx.set_tune({"sort_shift": 31})
+        ctx.upload(g)
+        r = ctx.run("ondemand")
+        assert np.array_equal(ctx.copy_k(r["triangle_count"]), o.k)
