@@ -78,7 +78,7 @@ def parse():
                    help="variant per request: by memory estimate (direct when it fits budget/direct_div) or on-demand")
     p.add_argument("--serve-direct-div", type=int, default=0)
     p.add_argument("--serve-budget-gb", type=float, default=0.0, help="server memory budget (0: the device's)")
-    p.add_argument("--serve-workers", type=int, default=2)
+    p.add_argument("--serve-workers", type=int, default=3)
     p.add_argument("--batch-master-seed", type=int, default=4)
     return p.parse_args()
 

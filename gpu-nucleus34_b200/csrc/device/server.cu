@@ -326,7 +326,7 @@ int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_o
 	if (opts)
 		s->opts = *opts;
 	s->opts.tune_table = nullptr; // read by each worker context as it is created; not kept
-	const uint32_t per_dev = (sopts && sopts->workers) ? sopts->workers : 2u;
+	const uint32_t per_dev = (sopts && sopts->workers) ? sopts->workers : 3u;
 	s->max_batch = (sopts && sopts->max_batch_graphs) ? sopts->max_batch_graphs : 256;
 	s->route = sopts ? sopts->route : NUCLEUS34_ROUTE_MEMORY;
 	s->direct_div = (sopts && sopts->direct_div) ? sopts->direct_div : DEFAULT_DIRECT_DIV;

@@ -615,7 +615,7 @@ def batch_decompose_devices(graphs, devices, mem_budget_bytes: int = 0, flags: i
 class Server:
     """nucleus34_server_*: continuous batching of decomposition requests."""
 
-    def __init__(self, device: int = 0, mem_budget_bytes: int = 0, workers: int = 2, max_batch_graphs: int = 256,
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0, workers: int = 3, max_batch_graphs: int = 256,
                  flags: int = 0, route: int = ROUTE_MEMORY, direct_div: int = 0, devices=None):
         """workers: concurrent passes per device slot; devices: slot ordinals
         (one may repeat), mem_budget_bytes applies to each slot; route and

@@ -368,7 +368,7 @@ typedef struct nucleus34_server_s *nucleus34_server;
 
 typedef struct
 {
-	uint32_t workers;             /* concurrent passes per device, 0 = 2 */
+	uint32_t workers;             /* concurrent passes per device, 0 = 3 */
 	uint64_t max_batch_graphs;    /* requests per pass, 0 = 256 */
 	uint32_t route;               /* NUCLEUS34_ROUTE_* */
 	uint32_t direct_div;          /* ROUTE_MEMORY: direct estimate <= budget / direct_div; 0 = default */
