@@ -68,6 +68,8 @@ def parse():
                    help="exactly one decomposition of the workload graph (for ncu captures); prints its record")
     p.add_argument("--peel-profile", action="store_true",
                    help="with --capture-run: per-step profiling mode (plain launches, per-round trace on stderr)")
+    p.add_argument("--host-loop", action="store_true",
+                   help="with --capture-run: the peel's host-driven replay graphs instead of the device loop")
     p.add_argument("--batch-graphs", type=int, default=4096)
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-max-edges", type=float, default=1e6)
@@ -556,7 +558,7 @@ def capture_run(a):
     those of that decomposition alone."""
     import nucleus34 as n34
     g = make_graph(n34, a.scale, a.edge_factor, a.seed)
-    flags = n34.OPT_PROFILE_PEEL if a.peel_profile else 0
+    flags = (n34.OPT_PROFILE_PEEL if a.peel_profile else 0) | (n34.OPT_HOST_LOOP if a.host_loop else 0)
     with n34.Context(flags=flags) as ctx:
         ctx.upload(g)
         r = ctx.run(a.variant)
