@@ -943,10 +943,11 @@ __device__ __forceinline__ void debit_thread_tri(uint32_t t, const Lists &L, Ctl
 template <uint32_t LANE_MAX>
 __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	CtlX *ctl, Frontier fr, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
-	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T)
+	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T,
+	bool chunked)
 {
-	if (ctl->c.done)
-		return;
+	if (ctl->c.done || (chunked && !fr.bits()))
+		return; // chunked: the warp kernel's lanes take the short lists too
 	const uint32_t cur = ctl->c.cur;
 	const int32_t level = int32_t(ctl->c.level);
 	uint32_t *Fn = fr.bits() ? nullptr : fr.next_list(cur);
@@ -963,7 +964,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	});
 }
 
-template <bool BITS, uint32_t LANE_MAX>
+template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false>
 __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
 	uint32_t *__restrict__ B1, uint64_t W, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
@@ -991,6 +992,46 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 	const uint32_t *F = ctl->c.cur ? F1 : F0;
 	const uint32_t *Bc = ctl->c.cur ? B1 : B0;
 	uint32_t word = 0; // bits of word fi not yet taken (bitmap mode)
+	if (!BITS && CHUNKED)
+	{
+		// Chunked schedule (list frontiers): a warp takes ch consecutive
+		// frontier triangles, its lanes load their records and spans at once
+		// (one dependent chain per chunk instead of one per triangle), lanes
+		// debit the short lists themselves, then the warp debits the long
+		// ones. ch doubles while every warp still gets two chunks, so small
+		// frontiers keep one triangle per warp.
+		const uint32_t lane = lane_id();
+		uint32_t ch = 1;
+		while (ch < 32 && uint64_t(ch) * 2 * nwarps <= nF)
+			ch <<= 1;
+		for (uint64_t base = warp * ch; base < nF; base += nwarps * ch)
+		{
+			const uint64_t i = base + lane;
+			const bool have = lane < ch && i < nF;
+			uint32_t t = 0;
+			Lists L{0, 0, 0, 0, 0, 0};
+			if (have)
+			{
+				t = F[i];
+				L = frontier_lists(t, tris, span);
+			}
+			const bool is_long = have && (L.a1 - L.a0 > LANE_MAX);
+			if (have && !is_long)
+				debit_thread_tri<LANE_MAX, false, false>(t, L, ctl, Fn, nullptr, third, itri, S, level, T);
+			uint32_t longs = __ballot_sync(FULL, is_long);
+			while (longs)
+			{
+				const uint32_t sl = __ffs(longs) - 1;
+				longs &= longs - 1;
+				const uint32_t tt = __shfl_sync(FULL, t, sl);
+				// its lists again (record and spans were just loaded: cache hits)
+				// rather than six more registers held across the long debits
+				const Lists LL = frontier_lists(tt, tris, span);
+				debit_warp_tri<false, false>(tt, LL, sm, ctl, Fn, nullptr, third, itri, S, level, T);
+			}
+		}
+		return;
+	}
 #if N34_DEBIT_CURSOR
 	// [cpos, cend): frontier positions (list) or bitmap words claimed by this
 	// warp; a claim takes CLAIM of them from the round's cursor (warp-uniform)
@@ -1612,9 +1653,11 @@ __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 // (LM); ev5 (profiling only) is recorded between them.
 template <uint32_t LM>
 void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool lean, CtlX *ctl, const Frontier &fr,
-						const uint32_t *tris, const Incidence &inc, int32_t *S, uint64_t T, cudaEvent_t ev5)
+						const uint32_t *tris, const Incidence &inc, int32_t *S, uint64_t T, cudaEvent_t ev5,
+						bool chunked)
 {
-	k_debit_flags_thread<LM><<<gscan, PEEL_THREADS, 0, st>>>(ctl, fr, tris, inc.span, inc.third, inc.tri, S, T);
+	k_debit_flags_thread<LM><<<gscan, PEEL_THREADS, 0, st>>>(ctl, fr, tris, inc.span, inc.third, inc.tri, S, T,
+															 chunked);
 	if (ev5)
 		cudaEventRecord(ev5, st);
 #if N34_DEBIT_CURSOR
@@ -1637,6 +1680,9 @@ void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool le
 	if (lean)
 		k_debit_flags_warp<true, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
 																	 inc.span, inc.third, inc.tri, S, T);
+	else if (chunked)
+		k_debit_flags_warp<false, LM, true><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W,
+																			tris, inc.span, inc.third, inc.tri, S, T);
 	else
 		k_debit_flags_warp<false, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
 																	  inc.span, inc.third, inc.tri, S, T);
@@ -1709,6 +1755,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 	// bits instead of two lists of T ids, and, when the caller passes K == S,
 	// k kept in S (a dead triangle holds -1 - k) and converted at the end.
 	const bool lean = flags && c.lean_run;
+	// chunked debit schedule (list frontiers) unless the split one is asked for
+	const bool chunked = !lean && !(c.opt_flags & NUCLEUS34_OPT_SPLIT_DEBIT);
 	const bool k_in_s = (K == S);
 	int32_t *Kw = k_in_s ? nullptr : K;
 	const uint64_t fwords = (T + 31) / 32;
@@ -1865,12 +1913,12 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				cudaEvent_t ev5 = ev ? ev[5] : nullptr;
 				static_assert(THREAD_MODE_MAX == TUNE_LANE_MAX, "default lane/warp split");
 				if (tn.lane_max == 8)
-					launch_debit_flags<8>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5);
+					launch_debit_flags<8>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked);
 				else if (tn.lane_max == 32)
-					launch_debit_flags<32>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5);
+					launch_debit_flags<32>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked);
 				else
 					launch_debit_flags<THREAD_MODE_MAX>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T,
-														ev5);
+														ev5, chunked);
 				tick(6);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, c.dsrc, c.dE, inc.span,
 																	   inc.third, inc.tpos, inc.tri, 3 * T);

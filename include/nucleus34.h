@@ -116,6 +116,12 @@ typedef struct
  * usually their longest list, become neighbours) instead of triangle-id
  * order. Results are identical. */
 #define NUCLEUS34_OPT_FRONTIER_BY_C 0x80u
+/* opts.flags: the earlier debit schedule of the death-flag peel, one thread
+ * per dying triangle with a short list and one warp per triangle with a long
+ * one (two kernels), instead of warps that take chunks of up to 32 frontier
+ * triangles, load their lists in parallel and debit short and long ones.
+ * Results are identical. */
+#define NUCLEUS34_OPT_SPLIT_DEBIT 0x100u
 
 typedef struct
 {
