@@ -34,6 +34,11 @@ reference takes its segmented path by its own rule. Scale 20 must be run with
     python oracle/ref_gpu_timing.py --scale 12 --seed 1 --program ondemand --kfile
     python oracle/ref_gpu_timing.py --scale 18 --program ondemand --kfile
     python oracle/ref_gpu_timing.py --scale 20 --program ondemand --kfile --free-gb 80
+    python oracle/ref_gpu_timing.py --graph rgg --n 4000000 --degree 48 --seed 3 --kdiff
+
+With --kdiff (on-demand) the reference's k file is not hashed but reduced to
+its k column by oracle/_build/kfile_column and compared with ours row by row:
+the differing rows, their triangles and their highest edge ids are reported.
 """
 import argparse
 import hashlib
@@ -166,6 +171,9 @@ def main():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--program", choices=["ondemand", "direct"], default="ondemand")
     ap.add_argument("--kfile", action="store_true", help="compare the k files (sha256 or multisets)")
+    ap.add_argument("--kdiff", action="store_true",
+                    help="on-demand: also compare the k files row by row (the reference's k column through "
+                         "oracle/_build/kfile_column) and report the differing rows and their edges")
     ap.add_argument("--ours-runs", type=int, default=3)
     ap.add_argument("--free-gb", type=float, default=0.0)
     ap.add_argument("--timeout", type=float, default=1200)
@@ -193,7 +201,16 @@ def main():
         out["vertices"], out["oriented_edges"] = int(g.n), int(g.m)
         # ---- reference ----
         side = None
-        ref_fifo = FifoHash(os.path.join(td, "ref.k"), keep_rows=a.program == "direct") if a.kfile else None
+        kcol_proc = None
+        if a.kdiff:
+            # the reference's k file goes through kfile_column (its k column to a file), not the hasher
+            fifo = os.path.join(td, "ref.k")
+            os.mkfifo(fifo)
+            tool = os.path.join(HERE, "_build", "kfile_column")
+            kcol_proc = subprocess.Popen([tool, fifo, os.path.join(td, "ref.k8")], stdout=subprocess.PIPE, text=True)
+            ref_fifo = None
+        else:
+            ref_fifo = FifoHash(os.path.join(td, "ref.k"), keep_rows=a.program == "direct") if a.kfile else None
         try:
             if a.free_gb > 0:
                 side = subprocess.Popen([sys.executable, "-c", SIDECAR, str(a.free_gb)], stdout=subprocess.PIPE,
@@ -203,7 +220,8 @@ def main():
             else:
                 out["mode"] = "the reference's own choice with the whole GPU free"
             # cuNucleus34 <dataset> [parts] [out]; cuNucleus34_ondemand <dataset> [out]
-            cmd = [exe, path] + (["1"] if a.program == "direct" else []) + ([ref_fifo.path] if ref_fifo else [])
+            kpath = ref_fifo.path if ref_fifo else (os.path.join(td, "ref.k") if kcol_proc else None)
+            cmd = [exe, path] + (["1"] if a.program == "direct" else []) + ([kpath] if kpath else [])
             with Clocks() as ck:
                 t0 = time.time()
                 r = subprocess.run(cmd, capture_output=True, text=True, timeout=a.timeout, env=env)
@@ -222,6 +240,16 @@ def main():
                 side.terminate()
                 side.wait(timeout=60)
         ref_sha = ref_fifo.finish() if ref_fifo else None
+        ref_k8 = None
+        if kcol_proc is not None:
+            if kcol_proc.poll() is None:  # the reference never opened its k file: unblock the reader
+                try:
+                    os.close(os.open(os.path.join(td, "ref.k"), os.O_WRONLY | os.O_NONBLOCK))
+                except OSError:
+                    pass
+            kcol_proc.wait(timeout=600)
+            import numpy as np
+            ref_k8 = np.fromfile(os.path.join(td, "ref.k8"), dtype=np.uint8)
         # ---- ours ----
         with n34.Context() as ctx:
             ctx.upload(g)
@@ -232,7 +260,10 @@ def main():
                     res = ctx.run(a.program)
                     runs.append(res)
             out["clocks_ours"] = ck.summary()
-            K = ctx.copy_k(int(res["triangle_count"]))
+            if ref_k8 is not None:
+                K, TR = ctx.copy_k(int(res["triangle_count"]), with_tris=True)
+            else:
+                K = ctx.copy_k(int(res["triangle_count"]))
         tt = [x["t_total"] for x in runs]
         res = runs[-1]
         ours = {"t_total_median": statistics.median(tt), "t_total_runs": tt,
@@ -241,7 +272,24 @@ def main():
                 "K_max": int(res["k_max"]), "K_avg": float(res["k_avg"]), "peak_device_bytes":
                 int(res["peak_device_bytes"])}
         out["ours"] = ours
-        if a.kfile:
+        if ref_k8 is not None:
+            import numpy as np
+            ours_k = K.astype(np.int64)
+            n_cmp = min(len(ref_k8), len(ours_k))
+            diff = np.flatnonzero(ref_k8[:n_cmp].astype(np.int64) != ours_k[:n_cmp])
+            dd = {"rows_reference": int(len(ref_k8)), "rows_ours": int(len(ours_k)), "rows_differing": int(len(diff))}
+            if len(diff):
+                top_edge = TR[diff].max(axis=1).astype(np.int64)
+                m = int(g.m)
+                dd["first"] = [{"row": int(i), "triangle": [int(x) for x in TR[i]], "k_reference": int(ref_k8[i]),
+                                "k_ours": int(ours_k[i])} for i in diff[:12]]
+                dd["oriented_edges"] = m
+                dd["highest_edge_of_differing_rows"] = {"min": int(top_edge.min()), "max": int(top_edge.max()),
+                                                        "within_last_1024_edges": int((top_edge >= m - 1024).sum())}
+                dd["k_reference_minus_ours"] = {str(v): int(c) for v, c in zip(*np.unique(
+                    ref_k8[diff].astype(np.int64) - ours_k[diff], return_counts=True))}
+            out["kdiff"] = dd
+        if a.kfile and ref_k8 is None:
             our_fifo = FifoHash(os.path.join(td, "ours.k"), keep_rows=a.program == "direct")
             try:
                 n34.decompose(g, variant=a.program, n_quds=0, kfile=our_fifo.path)
@@ -267,13 +315,16 @@ def main():
                 "K_avg": float(f"{ours['K_avg']:.6g}") == float(rec.get("K_avg", -1)),
                 "K_first": kref == [int(x) for x in K[: len(kref)]],
             }
-            if a.kfile:
+            if "kfile" in out:
                 kf = out["kfile"]
                 if a.program == "ondemand":
                     eq["kfile_sha256"] = kf["reference_sha256"] == kf["ours_sha256"]
                 else:
                     eq["kfile_rows_multiset"] = kf["reference_rows_sorted_sha256"] == kf["ours_rows_sorted_sha256"]
                     eq["kfile_k_multiset"] = kf["reference_k_sorted_sha256"] == kf["ours_k_sorted_sha256"]
+            if "kdiff" in out:
+                eq["kfile_rows"] = out["kdiff"]["rows_differing"] == 0 and \
+                    out["kdiff"]["rows_reference"] == out["kdiff"]["rows_ours"]
             out["equal"] = eq
             out["all_equal"] = all(eq.values())
             if rec.get("total_time_sec"):
