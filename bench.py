@@ -61,7 +61,7 @@ def parse():
     p.add_argument("--cpu-sample-scale", type=int, default=14)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="decompose", choices=["decompose", "batch", "serve", "variants"],
+    p.add_argument("--workload", default="decompose", choices=["decompose", "batch", "serve", "variants", "csr"],
                    help="decompose: the headline single-graph metric; batch: the batched form "
                         "(graphs/s of nucleus34_batch_decompose vs one decomposition per graph)")
     p.add_argument("--capture-run", action="store_true",
@@ -553,6 +553,41 @@ def run_variants(a):
     return 0
 
 
+def run_csr(a):
+    """The oriented CSR of an edge list built on the host
+    (nucleus34_graph_from_edges) and on the device
+    (nucleus34_ctx_upload_edges: pairs to the device, symmetrise, sort,
+    unique, orient there), RGG 4M points degree 48 seed 3 and R-MAT scale 20:
+    wall time of each (median of 3 after one warm-up), and the two CSRs
+    compared entry for entry."""
+    import numpy as np
+    import nucleus34 as n34
+    rows = []
+    for name, gen in (("RGG 4M degree 48 seed 3", lambda: n34.gen_rgg(4000000, 48.0, 3)),
+                      ("R-MAT scale 20 ef 16 seed 2", lambda: n34.gen_rmat(20, 16, 2))):
+        s, d = gen()
+        host, dev = [], []
+        g = None
+        for _ in range(4):
+            t0 = time.perf_counter()
+            g = n34.graph_from_edges(s, d)
+            host.append(time.perf_counter() - t0)
+        with n34.Context() as ctx:
+            for _ in range(4):
+                t0 = time.perf_counter()
+                n, m = ctx.upload_edges(s, d)
+                dev.append(time.perf_counter() - t0)
+            got = ctx.copy_csr()
+        same = (n, m) == (g.n, g.m) and np.array_equal(got.O, g.O[: g.n + 1]) and np.array_equal(got.E, g.E)
+        rows.append({"graph": name, "pairs": int(len(s)), "n": int(g.n), "m": int(g.m),
+                     "host_build_s": statistics.median(host[1:]), "device_build_s": statistics.median(dev[1:]),
+                     "host_threads": os.cpu_count(), "same_csr": bool(same)})
+        log(f"[bench] {name}: host {rows[-1]['host_build_s']:.3f} s, device {rows[-1]['device_build_s']:.3f} s, "
+            f"same {same}")
+    print(json.dumps({"metric": "oriented CSR build time", "unit": "s", "rows": rows}), flush=True)
+    return 0 if all(r["same_csr"] for r in rows) else 1
+
+
 def capture_run(a):
     """One decomposition and nothing else, so that ncu launch indices are
     those of that decomposition alone."""
@@ -598,6 +633,8 @@ def main():
         return run_serve(a)
     if a.workload == "variants":
         return run_variants(a)
+    if a.workload == "csr":
+        return run_csr(a)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(a.gpus)))
     local = int(os.environ.get("LOCAL_RANK", "0"))
