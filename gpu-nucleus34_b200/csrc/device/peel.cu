@@ -1755,8 +1755,9 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 	// bits instead of two lists of T ids, and, when the caller passes K == S,
 	// k kept in S (a dead triangle holds -1 - k) and converted at the end.
 	const bool lean = flags && c.lean_run;
-	// chunked debit schedule (list frontiers) unless the split one is asked for
-	const bool chunked = !lean && !(c.opt_flags & NUCLEUS34_OPT_SPLIT_DEBIT);
+	// chunked debit schedule (list frontiers) when asked for; the split one
+	// (a thread per short-list triangle, a warp per long one) by default
+	const bool chunked = !lean && (c.opt_flags & NUCLEUS34_OPT_CHUNKED_DEBIT);
 	const bool k_in_s = (K == S);
 	int32_t *Kw = k_in_s ? nullptr : K;
 	const uint64_t fwords = (T + 31) / 32;

@@ -420,7 +420,7 @@ OPT_HOST_RESULTS = 0x10
 OPT_HOST_LOOP = 0x20
 OPT_NO_SMALL_ROUNDS = 0x40
 OPT_FRONTIER_BY_C = 0x80
-OPT_SPLIT_DEBIT = 0x100
+OPT_CHUNKED_DEBIT = 0x100
 
 
 # The tune table the autotuner wrote on a B200 for this build's measured graph

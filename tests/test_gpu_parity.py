@@ -196,15 +196,15 @@ def test_frontier_ordered_by_c_edge_matches(n34, oracle, case):
 
 
 @pytest.mark.parametrize("case", [("rmat", 13, 16, 3), ("rgg", 30000, 40, 9)])
-def test_split_debit_schedule_matches(n34, oracle, case):
-    """The two-kernel debit schedule (a thread per short-list triangle, a
-    warp per long one) and the default chunked one give the oracle's k."""
+def test_chunked_debit_schedule_matches(n34, oracle, case):
+    """The default two-kernel debit schedule (a thread per short-list
+    triangle, a warp per long one) and the chunked one give the oracle's k."""
     if case[0] == "rmat":
         s, t = n34.gen_rmat(case[1], case[2], case[3])
     else:
         s, t = n34.gen_rgg(case[1], case[2], case[3])
     g = n34.graph_from_edges(s, t)
     o = oracle.decompose(g)
-    for fl in (0, n34.OPT_SPLIT_DEBIT, n34.OPT_SPLIT_DEBIT | n34.OPT_NO_SMALL_ROUNDS):
+    for fl in (0, n34.OPT_CHUNKED_DEBIT, n34.OPT_CHUNKED_DEBIT | n34.OPT_NO_SMALL_ROUNDS):
         d = n34.decompose(g, variant="ondemand", flags=fl, n_quds=0)
         assert np.array_equal(d.k, o.k), fl
