@@ -177,14 +177,13 @@ __device__ __forceinline__ void gather_take(const Frontier fr, CtlX *ctl, bool t
 	}
 }
 
-// Level-change scans with 16-byte loads (build option N34_SCAN_VEC=1): each
-// thread reads eight consecutive supports per step, two aligned int4 loads,
-// so that a warp keeps 1 KB in flight instead of 128 bytes; a warp appends to
-// the frontier only in steps where one of its lanes takes a triangle.
-#ifndef N34_SCAN_VEC
-#define N34_SCAN_VEC 0
-#endif
-#if N34_SCAN_VEC
+// Level-change scans. With vec (the default) each thread reads eight
+// consecutive supports per step as two aligned 16-byte loads, so that a warp
+// keeps 1 KB in flight instead of 128 bytes, and a warp appends its step's
+// takes with one atomic on the frontier counter (a warp scan of the lanes'
+// counts) instead of one ballot and atomic per 32 supports. Without vec:
+// one support per thread per step (kept for comparison,
+// NUCLEUS34_OPT_SCALAR_SCANS).
 constexpr uint32_t SCAN_VEC = 8;
 
 // v[j] = S[t0 + j] for t0 + j < T, else -1 (never taken); t0 is a multiple of
@@ -212,39 +211,66 @@ __device__ __forceinline__ void load_supports8(const int32_t *__restrict__ S, ui
 	}
 }
 
-// Appends every t in [t0, t0 + 8) whose support is in [0, hi] (all lanes call).
+// Appends every t whose support is in [0, hi] (all threads of the grid call).
 __device__ __forceinline__ void gather_range8(const Frontier fr, CtlX *ctl, const int32_t *__restrict__ S,
 											  uint64_t T, uint32_t hi)
 {
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x * SCAN_VEC;
+	const uint32_t lane = lane_id();
 	for (uint64_t b0 = uint64_t(blockIdx.x) * blockDim.x * SCAN_VEC; b0 < T; b0 += stride)
 	{
 		const uint64_t t0 = b0 + uint64_t(threadIdx.x) * SCAN_VEC;
 		int32_t v[SCAN_VEC];
 		load_supports8(S, T, t0, v);
-		bool any = false;
+		uint32_t mask = 0;
 #pragma unroll
 		for (uint32_t j = 0; j < SCAN_VEC; ++j)
-			any = any || (v[j] >= 0 && uint32_t(v[j]) <= hi);
-		if (!__any_sync(FULL, any))
+			if (v[j] >= 0 && uint32_t(v[j]) <= hi)
+				mask |= 1u << j;
+		const uint32_t cnt = __popc(mask);
+		uint32_t x = cnt; // inclusive warp scan of the counts
+#pragma unroll
+		for (uint32_t o = 1; o < 32; o <<= 1)
+		{
+			const uint32_t y = __shfl_up_sync(FULL, x, o);
+			if (lane >= o)
+				x += y;
+		}
+		const uint32_t total = __shfl_sync(FULL, x, 31);
+		if (total == 0)
 			continue; // warp-uniform: b0 is the same for the whole block
-#pragma unroll
-		for (uint32_t j = 0; j < SCAN_VEC; ++j)
-			gather_take(fr, ctl, v[j] >= 0 && uint32_t(v[j]) <= hi, t0 + j, T);
+		uint32_t base = 0;
+		if (lane == 31)
+			base = atomicAdd(&ctl->c.nF, total);
+		base = __shfl_sync(FULL, base, 31);
+		uint32_t pos = base + x - cnt;
+		while (mask)
+		{
+			const uint32_t j = __ffs(mask) - 1;
+			mask &= mask - 1;
+			const uint64_t t = t0 + j;
+			if (fr.bits())
+				atomicOr(fr.cur_bits(ctl->c.cur) + (t >> 5), 1u << (t & 31));
+			else if (pos < T)
+				fr.cur_list(ctl->c.cur)[pos] = uint32_t(t);
+			else
+				atomicOr(&ctl->c.error, 1u);
+			++pos;
+		}
 	}
 }
-#endif
 
 __global__ void __launch_bounds__(PEEL_THREADS) k_gather_next(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T,
-															  Frontier fr)
+															  Frontier fr, bool vec)
 {
 	if (ctl->c.done || !ctl->scan)
 		return;
 	const int32_t want = int32_t(ctl->c.level) + 1;
-#if N34_SCAN_VEC
-	gather_range8(fr, ctl, S, T, uint32_t(want));
-	return;
-#endif
+	if (vec)
+	{
+		gather_range8(fr, ctl, S, T, uint32_t(want));
+		return;
+	}
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < T; t0 += stride)
 	{
@@ -259,7 +285,8 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather_next(CtlX *ctl, const i
 	}
 }
 
-__global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T)
+__global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T,
+														   bool vec)
 {
 	if (ctl->c.done || !ctl->scan)
 		return;
@@ -271,26 +298,29 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int3
 	if (nf)
 		return;
 	uint32_t mn = INF;
-#if N34_SCAN_VEC
-	const uint64_t vstride = uint64_t(gridDim.x) * blockDim.x * SCAN_VEC;
-	for (uint64_t t0 = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * SCAN_VEC; t0 < T; t0 += vstride)
+	if (vec)
 	{
-		int32_t v[SCAN_VEC];
-		load_supports8(S, T, t0, v);
+		const uint64_t vstride = uint64_t(gridDim.x) * blockDim.x * SCAN_VEC;
+		for (uint64_t t0 = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) * SCAN_VEC; t0 < T; t0 += vstride)
+		{
+			int32_t v[SCAN_VEC];
+			load_supports8(S, T, t0, v);
 #pragma unroll
-		for (uint32_t j = 0; j < SCAN_VEC; ++j)
-			if (v[j] >= 0)
-				mn = min(mn, uint32_t(v[j]));
+			for (uint32_t j = 0; j < SCAN_VEC; ++j)
+				if (v[j] >= 0)
+					mn = min(mn, uint32_t(v[j]));
+		}
 	}
-#else
-	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-	for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
+	else
 	{
-		const int32_t s = S[t];
-		if (s >= 0)
-			mn = min(mn, uint32_t(s));
+		const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+		for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < T; t += stride)
+		{
+			const int32_t s = S[t];
+			if (s >= 0)
+				mn = min(mn, uint32_t(s));
+		}
 	}
-#endif
 #pragma unroll
 	for (int o = 16; o > 0; o >>= 1)
 		mn = min(mn, __shfl_xor_sync(FULL, mn, o));
@@ -300,7 +330,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_scan_min(CtlX *ctl, const int3
 
 // Second chance of the level change: gather at the minimum (or finish).
 __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_t *__restrict__ S, uint64_t T,
-														 Frontier fr)
+														 Frontier fr, bool vec)
 {
 	if (ctl->c.done || !ctl->scan)
 		return;
@@ -320,10 +350,11 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_gather(CtlX *ctl, const int32_
 	// every alive triangle sits above the old level, so the minimum is the new one
 	if (blockIdx.x == 0 && threadIdx.x == 0)
 		ctl->c.level = mn;
-#if N34_SCAN_VEC
-	gather_range8(fr, ctl, S, T, mn);
-	return;
-#endif
+	if (vec)
+	{
+		gather_range8(fr, ctl, S, T, mn);
+		return;
+	}
 	const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
 	for (uint64_t t0 = uint64_t(blockIdx.x) * blockDim.x; t0 < T; t0 += stride)
 	{
@@ -964,8 +995,10 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	});
 }
 
-template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false>
-__global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_warp(
+// The pipelined instantiation returns before the generic walk below.
+#pragma nv_diag_suppress 128
+template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false, bool PIPE = false>
+__global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
 	uint32_t *__restrict__ B1, uint64_t W, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
 	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T)
@@ -1029,6 +1062,45 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 				const Lists LL = frontier_lists(tt, tris, span);
 				debit_warp_tri<false, false>(tt, LL, sm, ctl, Fn, nullptr, third, itri, S, level, T);
 			}
+		}
+		return;
+	}
+	if (!BITS && PIPE)
+	{
+		// Software-pipelined walk of this warp's frontier positions: the id of
+		// the triangle two ahead and the record (three edge ids) of the one
+		// after the current are loaded before the current triangle's debit and
+		// used after it, so only the spans' load waits at the top of each step.
+		uint64_t fi = warp;
+		uint32_t tc = fi < nF ? F[fi] : 0;
+		uint32_t tn = fi + nwarps < nF ? F[fi + nwarps] : 0;
+		uint32_t ea = 0, eb = 0, ec = 0;
+		if (fi < nF)
+		{
+			ea = __ldg(tris + 3 * uint64_t(tc));
+			eb = __ldg(tris + 3 * uint64_t(tc) + 1);
+			ec = __ldg(tris + 3 * uint64_t(tc) + 2);
+		}
+		for (; fi < nF; fi += nwarps)
+		{
+			const uint64_t f2 = fi + 2 * nwarps;
+			const uint32_t t2 = f2 < nF ? F[f2] : 0;
+			uint32_t na = 0, nb = 0, nc = 0;
+			if (fi + nwarps < nF)
+			{
+				na = __ldg(tris + 3 * uint64_t(tn));
+				nb = __ldg(tris + 3 * uint64_t(tn) + 1);
+				nc = __ldg(tris + 3 * uint64_t(tn) + 2);
+			}
+			const uint2 sa = __ldg(span + ea), sb = __ldg(span + eb), sc = __ldg(span + ec);
+			const Lists L = order_lists(sa.x, sa.y, sb.x, sb.y, sc.x, sc.y);
+			if (L.a1 - L.a0 > LANE_MAX) // warp-uniform; short lists: the thread kernel
+				debit_warp_tri<false, false>(tc, L, sm, ctl, Fn, nullptr, third, itri, S, level, T);
+			tc = tn;
+			tn = t2;
+			ea = na;
+			eb = nb;
+			ec = nc;
 		}
 		return;
 	}
@@ -1100,6 +1172,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, N34_DEBIT_MINB) k_debit_flags_wa
 		debit_warp_tri<BITS, false>(t, L, sm, ctl, Fn, Bn, third, itri, S, level, T);
 	}
 }
+#pragma nv_diag_default 128
 
 // Ordering of large frontiers. Appends leave the next frontier in random
 // order; the debit of a random order reads every dying triangle's lists from
@@ -1654,7 +1727,7 @@ __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 template <uint32_t LM>
 void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool lean, CtlX *ctl, const Frontier &fr,
 						const uint32_t *tris, const Incidence &inc, int32_t *S, uint64_t T, cudaEvent_t ev5,
-						bool chunked)
+						bool chunked, bool pipelined)
 {
 	k_debit_flags_thread<LM><<<gscan, PEEL_THREADS, 0, st>>>(ctl, fr, tris, inc.span, inc.third, inc.tri, S, T,
 															 chunked);
@@ -1683,6 +1756,9 @@ void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool le
 	else if (chunked)
 		k_debit_flags_warp<false, LM, true><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W,
 																			tris, inc.span, inc.third, inc.tri, S, T);
+	else if (pipelined)
+		k_debit_flags_warp<false, LM, false, true><<<gwarp, PEEL_THREADS, 0, st>>>(
+			ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris, inc.span, inc.third, inc.tri, S, T);
 	else
 		k_debit_flags_warp<false, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
 																	  inc.span, inc.third, inc.tri, S, T);
@@ -1755,9 +1831,13 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 	// bits instead of two lists of T ids, and, when the caller passes K == S,
 	// k kept in S (a dead triangle holds -1 - k) and converted at the end.
 	const bool lean = flags && c.lean_run;
+	// level-change scans with vector loads unless the scalar ones are asked for
+	const bool vec_scans = !(c.opt_flags & NUCLEUS34_OPT_SCALAR_SCANS);
 	// chunked debit schedule (list frontiers) when asked for; the split one
 	// (a thread per short-list triangle, a warp per long one) by default
 	const bool chunked = !lean && (c.opt_flags & NUCLEUS34_OPT_CHUNKED_DEBIT);
+	// software-pipelined warp debit (list frontiers) when asked for
+	const bool pipelined = !lean && !chunked && (c.opt_flags & NUCLEUS34_OPT_PIPELINED_DEBIT);
 	const bool k_in_s = (K == S);
 	int32_t *Kw = k_in_s ? nullptr : K;
 	const uint64_t fwords = (T + 31) / 32;
@@ -1898,11 +1978,11 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 														 Kw, S, R, T, small_max);
 			}
 			tick(0);
-			k_gather_next<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, fr);
+			k_gather_next<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, fr, vec_scans);
 			tick(1);
-			k_scan_min<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T);
+			k_scan_min<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, vec_scans);
 			tick(2);
-			k_gather<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, fr);
+			k_gather<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, S, T, fr, vec_scans);
 			tick(3);
 			if (trace)
 				cudaMemcpyAsync(trace, &ctl->c, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream);
@@ -1914,12 +1994,14 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				cudaEvent_t ev5 = ev ? ev[5] : nullptr;
 				static_assert(THREAD_MODE_MAX == TUNE_LANE_MAX, "default lane/warp split");
 				if (tn.lane_max == 8)
-					launch_debit_flags<8>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked);
+					launch_debit_flags<8>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked,
+											pipelined);
 				else if (tn.lane_max == 32)
-					launch_debit_flags<32>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked);
+					launch_debit_flags<32>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked,
+											pipelined);
 				else
 					launch_debit_flags<THREAD_MODE_MAX>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T,
-														ev5, chunked);
+														ev5, chunked, pipelined);
 				tick(6);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, c.dsrc, c.dE, inc.span,
 																	   inc.third, inc.tpos, inc.tri, 3 * T);

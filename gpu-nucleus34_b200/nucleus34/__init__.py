@@ -421,6 +421,8 @@ OPT_HOST_LOOP = 0x20
 OPT_NO_SMALL_ROUNDS = 0x40
 OPT_FRONTIER_BY_C = 0x80
 OPT_CHUNKED_DEBIT = 0x100
+OPT_SCALAR_SCANS = 0x200
+OPT_PIPELINED_DEBIT = 0x400
 
 
 # The tune table the autotuner wrote on a B200 for this build's measured graph

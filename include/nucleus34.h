@@ -123,6 +123,15 @@ typedef struct
  * kernels). Results are identical; measured on one B200 it is 3% faster on
  * RGG 4M and 4.5% slower on R-MAT scale 20, so it is not the default. */
 #define NUCLEUS34_OPT_CHUNKED_DEBIT 0x100u
+/* opts.flags: the peel's level-change scans with one 4-byte load per thread
+ * per step and a ballot and atomic per 32 supports, instead of two 16-byte
+ * loads per thread per step and one atomic per warp step. Results are
+ * identical; kept for comparison. */
+#define NUCLEUS34_OPT_SCALAR_SCANS 0x200u
+/* opts.flags: the warp debit of the death-flag peel loads the next dying
+ * triangles' ids and records before the current one's debit (a software
+ * pipeline; 5 instead of 6 blocks per SM). Results are identical. */
+#define NUCLEUS34_OPT_PIPELINED_DEBIT 0x400u
 
 typedef struct
 {
