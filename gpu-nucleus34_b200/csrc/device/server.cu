@@ -66,9 +66,9 @@ struct Request
 	int status = NUCLEUS34_OK;
 	std::string error;
 	nucleus34_graph_summary summary{};
-	std::vector<int32_t> k;
-	std::vector<uint32_t> tris;
-	std::vector<uint32_t> quds;
+	std::vector<int32_t, NoInitAlloc<int32_t>> k;
+	HostU32 tris;
+	HostU32 quds;
 	clk::time_point t_submit, t_start, t_done;
 	uint64_t pass = 0; // pass that served it
 };
@@ -151,66 +151,66 @@ void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch, bool dire
 		c.seg_eoff = eoff;
 		rc = run(c, direct ? NUCLEUS34_DIRECT : NUCLEUS34_ONDEMAND, &r);
 	}
-	// results to the host: k of every request, triangle and clique lists of
-	// those that ask
-	bool want_tris = false, want_quds = false;
-	for (auto &q : batch)
+	// results to the host, each request's slices copied straight into its own
+	// buffers (left uninitialised until the copy): k of every request, the
+	// triangle and clique lists of those that ask
+	if (!rc)
 	{
-		want_tris = want_tris || (q->flags & NUCLEUS34_REQ_TRIANGLES);
-		want_quds = want_quds || (q->flags & NUCLEUS34_REQ_CLIQUES);
-	}
-	want_quds = want_quds && direct;
-	std::vector<int32_t> K;
-	std::vector<uint32_t> tris, quds;
-	if (!rc && c.T)
-	{
-		K.resize(c.T);
-		if (want_tris)
-			tris.resize(3 * c.T);
-		if (want_quds)
-			quds.resize(4 * c.Q);
-		if (cudaMemcpyAsync(K.data(), c.dK, c.T * 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess ||
-			(want_tris &&
-			 cudaMemcpyAsync(tris.data(), c.dtris, c.T * 12, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess) ||
-			(want_quds && c.Q &&
-			 cudaMemcpyAsync(quds.data(), c.dquds, c.Q * 16, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess) ||
-			cudaStreamSynchronize(c.stream) != cudaSuccess)
+		uint64_t q0 = 0; // first clique of request i in the union's list (cliques are listed by lowest triangle)
+		for (size_t i = 0; i < batch.size() && !rc; ++i)
+		{
+			Request &q = *batch[i];
+			const uint64_t t0 = c.seg_toff[i], T = c.seg_toff[i + 1] - t0;
+			const uint64_t Qi = c.seg_q[i];
+			q.summary.triangle_count = T;
+			q.summary.four_clique_count = Qi;
+			q.summary.k_max = c.seg_kmax[i];
+			q.summary.k_avg = T ? double(c.seg_ksum[i]) / double(T) : 0.0;
+			q.k.resize(T);
+			if (q.flags & NUCLEUS34_REQ_TRIANGLES)
+				q.tris.resize(3 * T);
+			if (direct && (q.flags & NUCLEUS34_REQ_CLIQUES))
+				q.quds.resize(4 * Qi);
+			if ((T && cudaMemcpyAsync(q.k.data(), c.dK + t0, T * 4, cudaMemcpyDeviceToHost, c.stream) != cudaSuccess) ||
+				(T && !q.tris.empty() &&
+				 cudaMemcpyAsync(q.tris.data(), c.dtris + 3 * t0, T * 12, cudaMemcpyDeviceToHost, c.stream) !=
+					 cudaSuccess) ||
+				(Qi && !q.quds.empty() &&
+				 cudaMemcpyAsync(q.quds.data(), c.dquds + 4 * q0, Qi * 16, cudaMemcpyDeviceToHost, c.stream) !=
+					 cudaSuccess))
+				rc = fail(NUCLEUS34_E_CUDA, "serving: result copy");
+			q0 += Qi;
+		}
+		if (!rc && cudaStreamSynchronize(c.stream) != cudaSuccess)
 			rc = fail(NUCLEUS34_E_CUDA, "serving: result copy");
 	}
+	// a finished pass holds nothing on the device (admission counts on it)
+	const std::vector<uint64_t> toff = std::move(c.seg_toff);
+	c.release_results();
+	c.release_graph();
+	// ids of the union back to each request's own (edge ids, triangle ids)
 	const std::string err = rc ? std::string(nucleus34_last_error()) : std::string();
-	uint64_t q0 = 0; // first clique of request i in the union's list (cliques are listed by lowest triangle)
 	for (size_t i = 0; i < batch.size(); ++i)
 	{
 		Request &q = *batch[i];
 		q.status = rc;
 		q.error = err;
 		if (rc)
-			continue;
-		const uint64_t t0 = c.seg_toff[i], T = c.seg_toff[i + 1] - t0;
-		const uint64_t Qi = c.seg_q[i];
-		q.summary.triangle_count = T;
-		q.summary.four_clique_count = Qi;
-		q.summary.k_max = c.seg_kmax[i];
-		q.summary.k_avg = T ? double(c.seg_ksum[i]) / double(T) : 0.0;
-		q.k.assign(K.begin() + t0, K.begin() + t0 + T);
-		if (q.flags & NUCLEUS34_REQ_TRIANGLES)
 		{
-			q.tris.assign(tris.begin() + 3 * t0, tris.begin() + 3 * (t0 + T));
-			const uint32_t eo = uint32_t(eoff[i]);
+			decltype(q.k)().swap(q.k);
+			decltype(q.tris)().swap(q.tris);
+			decltype(q.quds)().swap(q.quds);
+			continue;
+		}
+		const uint32_t eo = uint32_t(eoff[i]);
+		if (eo)
 			for (auto &x : q.tris)
 				x -= eo;
-		}
-		if (want_quds && (q.flags & NUCLEUS34_REQ_CLIQUES))
-		{
-			q.quds.assign(quds.begin() + 4 * q0, quds.begin() + 4 * (q0 + Qi));
+		const uint32_t to = uint32_t(toff[i]);
+		if (to)
 			for (auto &x : q.quds)
-				x -= uint32_t(t0);
-		}
-		q0 += Qi;
+				x -= to;
 	}
-	// a finished pass holds nothing on the device (admission counts on it)
-	c.release_results();
-	c.release_graph();
 }
 
 void worker_loop(nucleus34_server_s *s, size_t wi)
