@@ -81,6 +81,8 @@ def parse():
     p.add_argument("--serve-direct-div", type=int, default=0)
     p.add_argument("--serve-budget-gb", type=float, default=0.0, help="server memory budget (0: the device's)")
     p.add_argument("--serve-workers", type=int, default=3)
+    p.add_argument("--serve-concurrent-runs", type=int, default=0,
+                   help="decompositions running at once per device slot (0: no limit)")
     p.add_argument("--batch-master-seed", type=int, default=4)
     return p.parse_args()
 
@@ -458,7 +460,7 @@ def run_serve(a):
         if tdist:
             tdist.barrier()
         with n34.Server(device=dev, mem_budget_bytes=budget, workers=a.serve_workers, route=route,
-                        direct_div=a.serve_direct_div) as srv:
+                        direct_div=a.serve_direct_div, concurrent_runs=a.serve_concurrent_runs) as srv:
             ids = {}
             w0 = time.perf_counter()
             for i in share:
@@ -511,6 +513,7 @@ def run_serve(a):
         "config": {"workload": f"{n_all} requests, Poisson arrivals, half R-MAT half RGG (degree 16..64), undirected "
                                f"edges log-uniform 1e3..{a.serve_max_edges:.0e}, master seed {a.serve_master_seed}",
                    "serial_plain_capacity_per_s": cap, "route": a.serve_route, "workers": a.serve_workers,
+                   "concurrent_runs": a.serve_concurrent_runs,
                    "budget_bytes": budget or "device", "parallelism": f"replicas x{world}"},
         "sweep": sweeps, "k_mismatched_requests": mism,
     }

@@ -89,6 +89,7 @@ struct Slot
 	int device = 0;
 	uint64_t budget = 0;
 	uint64_t in_flight = 0;
+	uint32_t running = 0; // passes inside their decomposition
 };
 
 } // namespace
@@ -100,8 +101,9 @@ struct nucleus34_server_s
 	uint64_t max_batch = 256;     // graphs per pass
 	uint32_t route = NUCLEUS34_ROUTE_MEMORY;
 	uint32_t direct_div = DEFAULT_DIRECT_DIV;
+	uint32_t max_running = 0;     // decompositions at once per slot, 0 = no limit
 	std::mutex mu;
-	std::condition_variable cv_work, cv_done;
+	std::condition_variable cv_work, cv_done, cv_run;
 	std::deque<std::shared_ptr<Request>> pending;
 	std::map<uint64_t, std::shared_ptr<Request>> all;
 	uint64_t next_id = 1, passes = 0, served = 0, direct_served = 0, busy_workers = 0;
@@ -129,8 +131,28 @@ void out_bounds(const uint32_t *D, uint64_t n, uint64_t &wedges, uint64_t &tripl
 	}
 }
 
+// Entry to and exit from a slot's decompositions (at most max_running at
+// once when set). The union build, upload and result copies stay outside, so
+// one worker prepares or drains a pass while another computes.
+void run_enter(nucleus34_server_s *s, Slot &slot)
+{
+	std::unique_lock<std::mutex> lk(s->mu);
+	s->cv_run.wait(lk, [&] { return s->max_running == 0 || slot.running < s->max_running; });
+	slot.running++;
+}
+
+void run_exit(nucleus34_server_s *s, Slot &slot)
+{
+	{
+		std::lock_guard<std::mutex> lk(s->mu);
+		slot.running--;
+	}
+	s->cv_run.notify_all();
+}
+
 // one pass over a set of requests of one variant (their union) on context c
-void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch, bool direct)
+void serve_union(nucleus34_server_s *s, Slot &slot, Ctx &c, std::vector<std::shared_ptr<Request>> &batch,
+				 bool direct)
 {
 	std::vector<nucleus34_csr> csrs(batch.size());
 	for (size_t i = 0; i < batch.size(); ++i)
@@ -149,7 +171,9 @@ void serve_union(Ctx &c, std::vector<std::shared_ptr<Request>> &batch, bool dire
 	if (!rc)
 	{
 		c.seg_eoff = eoff;
+		run_enter(s, slot);
 		rc = run(c, direct ? NUCLEUS34_DIRECT : NUCLEUS34_ONDEMAND, &r);
+		run_exit(s, slot);
 	}
 	// results to the host, each request's slices copied straight into its own
 	// buffers (left uninitialised until the copy): k of every request, the
@@ -274,7 +298,7 @@ void worker_loop(nucleus34_server_s *s, size_t wi)
 			for (auto &q : batch)
 				q->t_start = now;
 		}
-		serve_union(c, batch, direct);
+		serve_union(s, slot, c, batch, direct);
 		{
 			std::lock_guard<std::mutex> lk(s->mu);
 			slot.in_flight -= take_bytes;
@@ -330,6 +354,7 @@ int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_o
 	s->max_batch = (sopts && sopts->max_batch_graphs) ? sopts->max_batch_graphs : 256;
 	s->route = sopts ? sopts->route : NUCLEUS34_ROUTE_MEMORY;
 	s->direct_div = (sopts && sopts->direct_div) ? sopts->direct_div : DEFAULT_DIRECT_DIV;
+	s->max_running = sopts ? sopts->concurrent_runs : 0;
 	std::vector<int> devs;
 	if (sopts && sopts->device_count)
 		devs.assign(sopts->devices, sopts->devices + sopts->device_count);

@@ -135,7 +135,8 @@ class GraphSummary(C.Structure):
 
 class ServerOpts(C.Structure):
     _fields_ = [("workers", C.c_uint32), ("max_batch_graphs", C.c_uint64), ("route", C.c_uint32),
-                ("direct_div", C.c_uint32), ("device_count", C.c_uint32), ("devices", C.POINTER(C.c_int))]
+                ("direct_div", C.c_uint32), ("device_count", C.c_uint32), ("devices", C.POINTER(C.c_int)),
+                ("concurrent_runs", C.c_uint32)]
 
 
 class RequestInfo(C.Structure):
@@ -423,6 +424,7 @@ OPT_FRONTIER_BY_C = 0x80
 OPT_CHUNKED_DEBIT = 0x100
 OPT_SCALAR_SCANS = 0x200
 OPT_PIPELINED_DEBIT = 0x400
+OPT_DEBIT_TILES64 = 0x800
 
 
 # The tune table the autotuner wrote on a B200 for this build's measured graph
@@ -619,15 +621,18 @@ class Server:
     """nucleus34_server_*: continuous batching of decomposition requests."""
 
     def __init__(self, device: int = 0, mem_budget_bytes: int = 0, workers: int = 3, max_batch_graphs: int = 256,
-                 flags: int = 0, route: int = ROUTE_MEMORY, direct_div: int = 0, devices=None):
+                 flags: int = 0, route: int = ROUTE_MEMORY, direct_div: int = 0, devices=None,
+                 concurrent_runs: int = 0):
         """workers: concurrent passes per device slot; devices: slot ordinals
         (one may repeat), mem_budget_bytes applies to each slot; route and
-        direct_div: the variant chosen per request by its memory estimate."""
+        direct_div: the variant chosen per request by its memory estimate;
+        concurrent_runs: decompositions running at once per slot (0: no
+        limit)."""
         self._L = lib()
         opts = make_opts(device, mem_budget_bytes, flags=flags)
         self._devs = (C.c_int * len(devices))(*devices) if devices else None
         so = ServerOpts(workers, max_batch_graphs, route, direct_div, len(devices) if devices else 0,
-                        C.cast(self._devs, C.POINTER(C.c_int)) if devices else None)
+                        C.cast(self._devs, C.POINTER(C.c_int)) if devices else None, concurrent_runs)
         self._h = C.c_void_p()
         _check(self._L.nucleus34_server_create(C.byref(opts), C.byref(so), C.byref(self._h)), "server_create")
 

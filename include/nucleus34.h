@@ -132,6 +132,10 @@ typedef struct
  * triangles' ids and records before the current one's debit (a software
  * pipeline; 5 instead of 6 blocks per SM). Results are identical. */
 #define NUCLEUS34_OPT_PIPELINED_DEBIT 0x400u
+/* opts.flags: the warp debit of the death-flag peel merges the two shortest
+ * lists in tiles of 64 entries (two per lane) instead of 32, halving the
+ * dependent load steps on long lists. Results are identical. */
+#define NUCLEUS34_OPT_DEBIT_TILES64 0x800u
 
 typedef struct
 {
@@ -390,6 +394,8 @@ typedef struct
 	uint32_t direct_div;          /* ROUTE_MEMORY: direct estimate <= budget / direct_div; 0 = default */
 	uint32_t device_count;        /* 0: opts.device alone; else devices[0..device_count) */
 	const int *devices;           /* ordinals (one may repeat: several budgets on one GPU) */
+	uint32_t concurrent_runs;     /* decompositions running at once per slot (the other workers
+	                               * build unions and copy results meanwhile); 0 = no limit */
 } nucleus34_server_opts;
 
 typedef struct

@@ -166,6 +166,20 @@ def test_two_device_slots_serve_every_request(n34):
         assert st["budget_bytes"] == 2 * (6 << 30)
 
 
+def test_one_run_at_a_time_serves_every_request(n34, oracle):
+    """With concurrent_runs = 1 the workers still build unions and copy
+    results concurrently, but one decomposition runs at a time on the slot;
+    every request (both variants) gets the result of its graph alone."""
+    graphs = _mixed_graphs(n34, 14, 21)
+    with n34.Server(workers=3, max_batch_graphs=4, concurrent_runs=1) as srv:
+        ids = [srv.submit(g) for g in graphs]
+        for g, rid in zip(graphs, ids):
+            info = srv.wait(rid, timeout_ms=300000)
+            assert np.array_equal(srv.copy_k(rid, info["triangle_count"]), oracle.decompose(g).k)
+        st = srv.stats()
+        assert st["served"] == len(graphs) and st["passes"] >= len(graphs) // 4
+
+
 def test_admission_estimates_bound_measured_peaks(n34):
     """The per-edge, per-wedge and per-triple constants bound the measured
     peak device bytes of each variant (the peak counts every allocation of
