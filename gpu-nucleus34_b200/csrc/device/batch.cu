@@ -449,15 +449,18 @@ int nucleus34_batch_decompose(const nucleus34_csr *graphs, uint64_t count, const
 			destroy_ctx(ctx0);
 			return finish(rc);
 		}
-		// chunks: greedy in graph order, 3T < 2^32 entry positions each, and
-		// about PASS_BYTES_PER_TRIANGLE bytes of a pass's peak per triangle
-		// within the memory budget (a single graph over that still runs alone)
+		// chunks: greedy in graph order, 3T < 2^32 entry positions each, at
+		// most FLAG_PEEL_MAX_TRIANGLES (so that every pass of several graphs
+		// peels with death flags), and about PASS_BYTES_PER_TRIANGLE bytes of a
+		// pass's peak per triangle within the memory budget (a single graph
+		// over that still runs alone)
 		constexpr uint64_t PASS_BYTES_PER_TRIANGLE = 80;
 		const uint64_t range_limit = 0xffffffffull / 3;
 		const uint64_t csr_bytes = 4 * (voff[count] + 1) + 8 * eoff[count];
 		const uint64_t budget = ctx0->c.budget;
 		const uint64_t mem_limit = budget > csr_bytes ? (budget - csr_bytes) / PASS_BYTES_PER_TRIANGLE : 0;
-		const uint64_t limit = std::max<uint64_t>(1, std::min(range_limit, mem_limit));
+		const uint64_t limit =
+			std::max<uint64_t>(1, std::min(std::min(range_limit, FLAG_PEEL_MAX_TRIANGLES), mem_limit));
 		std::vector<uint64_t> cut{0};
 		uint64_t acc = 0;
 		for (uint64_t g = 0; g < count; ++g)

@@ -131,6 +131,8 @@ __device__ __forceinline__ WarpSample warp_sample(const uint32_t *__restrict__ a
 
 // Lower bounds in [lo, hi) using a sample taken over [lo0, hi) with lo0 <= lo
 // (every entry before lo is below every x searched now). Called by all lanes.
+// W4: the per-lane search within the sample slice takes four-way steps.
+template <bool W4 = false>
 __device__ __forceinline__ uint32_t sampled_lower_bound(const uint32_t *__restrict__ a, const WarpSample &s,
 														uint32_t lo, uint32_t hi, bool want, uint32_t x)
 {
@@ -163,7 +165,7 @@ __device__ __forceinline__ uint32_t sampled_lower_bound(const uint32_t *__restri
 	}
 	uint32_t r = hi;
 	if (want)
-		r = lower_bound32(a, l, h, x);
+		r = W4 ? lower_bound32_w4(a, l, h, x) : lower_bound32(a, l, h, x);
 	return r;
 }
 
@@ -216,66 +218,6 @@ __device__ __forceinline__ void warp_merge2(const uint32_t *__restrict__ third, 
 	}
 }
 
-// Warp tile merge of A and B with 64-entry tiles (two entries per lane): on
-// long lists half the dependent steps of warp_merge2, for latency-bound
-// callers. Same contract as warp_merge2; f is called twice per step, for the
-// first and then the second 32 entries of the A tile, so common x still come
-// in ascending order.
-template <bool WITH_TRI, class F, bool COH = false>
-__device__ __forceinline__ void warp_merge2_64(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
-											   uint32_t a0, uint32_t a1, uint32_t b0, uint32_t b1, F &&f)
-{
-	const uint32_t lane = lane_id();
-	constexpr uint32_t NONE = 0xffffffffu;
-	while (a0 < a1 && b0 < b1) // warp-uniform
-	{
-		const uint32_t ai0 = a0 + lane, ai1 = a0 + 32 + lane, bi0 = b0 + lane, bi1 = b0 + 32 + lane;
-		const bool a0k = ai0 < a1, a1k = ai1 < a1, b0k = bi0 < b1, b1k = bi1 < b1;
-		const uint32_t av0 = a0k ? __ldg(third + ai0) : NONE, av1 = a1k ? __ldg(third + ai1) : NONE;
-		const uint32_t bv0 = b0k ? __ldg(third + bi0) : NONE, bv1 = b1k ? __ldg(third + bi1) : NONE;
-		uint32_t at0 = 0, at1 = 0, bt0 = 0, bt1 = 0;
-		if (WITH_TRI)
-		{
-			at0 = a0k ? ld_tri<COH>(itri + ai0) : 0u;
-			at1 = a1k ? ld_tri<COH>(itri + ai1) : 0u;
-			bt0 = b0k ? ld_tri<COH>(itri + bi0) : 0u;
-			bt1 = b1k ? ld_tri<COH>(itri + bi1) : 0u;
-		}
-		const uint32_t amax = __shfl_sync(FULL, av1, 31), bmax = __shfl_sync(FULL, bv1, 31);
-		const uint32_t m = amax < bmax ? amax : bmax;
-		const uint32_t b31 = __shfl_sync(FULL, bv0, 31); // tile entry 31
-#pragma unroll 1
-		for (uint32_t h = 0; h < 2; ++h)
-		{
-			const uint32_t av = h ? av1 : av0;
-			const bool ok = h ? a1k : a0k;
-			// first entry j of the 64-entry B tile with tile[j] >= av (63 if none)
-			uint32_t pos = b31 < av ? 32u : 0u;
-#pragma unroll
-			for (uint32_t step = 16; step > 0; step >>= 1)
-			{
-				const uint32_t j = pos + step - 1;
-				const uint32_t lo = __shfl_sync(FULL, bv0, j & 31), hi = __shfl_sync(FULL, bv1, j & 31);
-				if ((j >= 32 ? hi : lo) < av)
-					pos += step;
-			}
-			const uint32_t hlo = __shfl_sync(FULL, bv0, pos & 31), hhi = __shfl_sync(FULL, bv1, pos & 31);
-			const uint32_t hitv = pos >= 32 ? hhi : hlo;
-			uint32_t qb = 0;
-			if (WITH_TRI)
-			{
-				const uint32_t tlo = __shfl_sync(FULL, bt0, pos & 31), thi = __shfl_sync(FULL, bt1, pos & 31);
-				qb = pos >= 32 ? thi : tlo;
-			}
-			const bool found = ok && av <= m && hitv == av && b0 + pos < b1;
-			f(found, av, h ? ai1 : ai0, b0 + pos, h ? at1 : at0, qb);
-		}
-		// everything <= m is consumed; at least one tile is used up entirely
-		a0 += __popc(__ballot_sync(FULL, a0k && av0 <= m)) + __popc(__ballot_sync(FULL, a1k && av1 <= m));
-		b0 += __popc(__ballot_sync(FULL, b0k && bv0 <= m)) + __popc(__ballot_sync(FULL, b1k && bv1 <= m));
-	}
-}
-
 // Warp binary search of A's entries in B (B much longer than A).
 template <bool WITH_TRI, class F, bool COH = false>
 __device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
@@ -300,19 +242,13 @@ __device__ __forceinline__ void warp_search2(const uint32_t *__restrict__ third,
 	}
 }
 
-// Warp dispatch between merge and search for the two shortest lists (T64:
-// the merge takes 64-entry tiles).
-template <bool WITH_TRI = false, bool COH = false, bool T64 = false, class F>
+// Warp dispatch between merge and search for the two shortest lists.
+template <bool WITH_TRI = false, bool COH = false, class F>
 __device__ __forceinline__ void warp_intersect2(const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri,
 												const Lists &L, F &&f)
 {
 	if (use_merge(L))
-	{
-		if (T64)
-			warp_merge2_64<WITH_TRI, F &, COH>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
-		else
-			warp_merge2<WITH_TRI, F &, COH>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
-	}
+		warp_merge2<WITH_TRI, F &, COH>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
 	else
 		warp_search2<WITH_TRI, F &, COH>(third, itri, L.a0, L.a1, L.b0, L.b1, f);
 }

@@ -599,6 +599,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_direct(
 constexpr uint32_t DEAD = INC_DEAD;
 constexpr uint32_t DYING = 0x40000000u;
 constexpr uint32_t ID_MASK = 0x3fffffffu;
+static_assert(ID_MASK == FLAG_PEEL_MAX_TRIANGLES, "death-flag id range");
 
 // positions of triangle t's three entries: under b (third w), a (third v), c (third u);
 // read from tpos when the incidence keeps them, else searched
@@ -709,9 +710,6 @@ __device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q
 #ifndef N34_DEBIT_MINB
 #define N34_DEBIT_MINB 6
 #endif
-#ifndef N34_T64_MINB
-#define N34_T64_MINB 5
-#endif
 #if N34_DEBIT_CURSOR
 // Claims the next `claim` positions below cap from *cursor into [cpos, cend);
 // false when none are left. Called by all lanes with warp-uniform values.
@@ -748,7 +746,7 @@ struct DebitSmem
 // 32 live cliques instead of once per merge step that has any. Next-frontier
 // appends go to the list Fn (or bitmap Bn with BITS). COH: the flags are read
 // through L2 (a kernel that wrote them earlier in the same launch).
-template <bool BITS, bool COH, bool T64 = false>
+template <bool BITS, bool COH, bool W4 = false>
 __device__ __forceinline__ void debit_warp_tri(uint32_t t, const Lists &L, const DebitSmem &sm, CtlX *ctl,
 											   uint32_t *__restrict__ Fn, uint32_t *__restrict__ Bn,
 											   const uint32_t *__restrict__ third, const uint32_t *itri,
@@ -836,7 +834,7 @@ __device__ __forceinline__ void debit_warp_tri(uint32_t t, const Lists &L, const
 		else
 #endif
 		{
-			pc = sampled_lower_bound(third, cs, lo_c, L.c1, v, x);
+			pc = sampled_lower_bound<W4>(third, cs, lo_c, L.c1, v, x);
 			if (v && pc < L.c1)
 			{
 				xc = __ldg(third + pc);
@@ -872,7 +870,7 @@ __device__ __forceinline__ void debit_warp_tri(uint32_t t, const Lists &L, const
 		}
 		__syncwarp();
 	};
-	warp_intersect2<true, COH, T64>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
+	warp_intersect2<true, COH>(third, itri, L, [&](bool found, uint32_t x, uint32_t, uint32_t, uint32_t qa,
 												   uint32_t qb) {
 		n_steps += st;
 		// a clique is looked up on C only if its partners on A and B are
@@ -1000,8 +998,8 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 
 // The pipelined instantiation returns before the generic walk below.
 #pragma nv_diag_suppress 128
-template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false, bool PIPE = false, bool T64 = false>
-__global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : (T64 ? N34_T64_MINB : N34_DEBIT_MINB)) k_debit_flags_warp(
+template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false, bool PIPE = false, bool W4 = false>
+__global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
 	uint32_t *__restrict__ B1, uint64_t W, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
 	const uint32_t *__restrict__ third, const uint32_t *__restrict__ itri, int32_t *__restrict__ S, uint64_t T)
@@ -1172,7 +1170,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : (T64 ? N34_T64_MINB :
 		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 <= LANE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
-		debit_warp_tri<BITS, false, T64>(t, L, sm, ctl, Fn, Bn, third, itri, S, level, T);
+		debit_warp_tri<BITS, false, W4>(t, L, sm, ctl, Fn, Bn, third, itri, S, level, T);
 	}
 }
 #pragma nv_diag_default 128
@@ -1730,7 +1728,7 @@ __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 template <uint32_t LM>
 void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool lean, CtlX *ctl, const Frontier &fr,
 						const uint32_t *tris, const Incidence &inc, int32_t *S, uint64_t T, cudaEvent_t ev5,
-						bool chunked, bool pipelined, bool tiles64)
+						bool chunked, bool pipelined, bool wide4)
 {
 	k_debit_flags_thread<LM><<<gscan, PEEL_THREADS, 0, st>>>(ctl, fr, tris, inc.span, inc.third, inc.tri, S, T,
 															 chunked);
@@ -1762,7 +1760,7 @@ void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool le
 	else if (pipelined)
 		k_debit_flags_warp<false, LM, false, true><<<gwarp, PEEL_THREADS, 0, st>>>(
 			ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris, inc.span, inc.third, inc.tri, S, T);
-	else if (tiles64)
+	else if (wide4)
 		k_debit_flags_warp<false, LM, false, false, true><<<gwarp, PEEL_THREADS, 0, st>>>(
 			ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris, inc.span, inc.third, inc.tri, S, T);
 	else
@@ -1844,8 +1842,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 	const bool chunked = !lean && (c.opt_flags & NUCLEUS34_OPT_CHUNKED_DEBIT);
 	// software-pipelined warp debit (list frontiers) when asked for
 	const bool pipelined = !lean && !chunked && (c.opt_flags & NUCLEUS34_OPT_PIPELINED_DEBIT);
-	// 64-entry merge tiles in the warp debit (list frontiers) when asked for
-	const bool tiles64 = !lean && !chunked && !pipelined && (c.opt_flags & NUCLEUS34_OPT_DEBIT_TILES64);
+	// four-way searches for the warp debit's lookups on the longest list
+	const bool wide4 = !lean && !chunked && !pipelined && (c.opt_flags & NUCLEUS34_OPT_DEBIT_WIDE_SEARCH);
 	const bool k_in_s = (K == S);
 	int32_t *Kw = k_in_s ? nullptr : K;
 	const uint64_t fwords = (T + 31) / 32;
@@ -2003,13 +2001,13 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				static_assert(THREAD_MODE_MAX == TUNE_LANE_MAX, "default lane/warp split");
 				if (tn.lane_max == 8)
 					launch_debit_flags<8>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked,
-											pipelined, tiles64);
+											pipelined, wide4);
 				else if (tn.lane_max == 32)
 					launch_debit_flags<32>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked,
-											pipelined, tiles64);
+											pipelined, wide4);
 				else
 					launch_debit_flags<THREAD_MODE_MAX>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T,
-														ev5, chunked, pipelined, tiles64);
+														ev5, chunked, pipelined, wide4);
 				tick(6);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, c.dsrc, c.dE, inc.span,
 																	   inc.third, inc.tpos, inc.tri, 3 * T);

@@ -23,6 +23,10 @@ struct Incidence
 // Bit of an incidence entry's tri word that marks a peeled triangle (on-demand
 // peel with death flags; the incidence is discarded after the peel).
 constexpr uint32_t INC_DEAD = 0x80000000u;
+// Most triangles the on-demand peel keeps its death flags in the incidence
+// for (ids leave the top two bits of a tri word free); above it the slower
+// round-stamp peel runs. Union passes (batched form, serving) are cut below it.
+constexpr uint64_t FLAG_PEEL_MAX_TRIANGLES = 0x3fffffffull;
 
 // Triangle -> four-clique incidence of the direct variant.
 struct CliqueCsr

@@ -5,7 +5,8 @@
 // slot; a slot is a device with its own memory budget, and several slots may
 // name one GPU. A worker takes the pending requests in arrival order that fit
 // the memory still free in its slot (estimated per request from its CSR) and
-// within the 32-bit ranges (same-variant requests further back in the queue
+// within the 32-bit ranges, on-demand unions also within the 2^30 triangles
+// of the death-flag peel (same-variant requests further back in the queue
 // join too, past requests of the other variant), decomposes them in one pass
 // as a disjoint union
 // (the batched form), copies every request's results to the host and signals
@@ -243,6 +244,8 @@ void worker_loop(nucleus34_server_s *s, size_t wi)
 	Slot &slot = s->slots[s->worker_slot[wi]];
 	cudaSetDevice(c.device);
 	const uint64_t range_limit = 0xffffffffull / 3; // 3T incidence entries in 32-bit positions
+	// on-demand unions stay within the death-flag peel's triangle range
+	const uint64_t ondemand_limit = std::min(range_limit, FLAG_PEEL_MAX_TRIANGLES);
 	const uint64_t clique_limit = 0xffffffffull;     // direct: clique ids in 32 bits
 	for (;;)
 	{
@@ -280,7 +283,7 @@ void worker_loop(nucleus34_server_s *s, size_t wi)
 			{
 				auto &q = s->pending[i];
 				if (q->direct != direct || take_bytes + q->est_bytes > free_b ||
-					tri_bound + q->est_triangles > range_limit ||
+					tri_bound + q->est_triangles > (direct ? range_limit : ondemand_limit) ||
 					(direct && clique_bound + q->est_cliques > clique_limit))
 				{
 					++i;
