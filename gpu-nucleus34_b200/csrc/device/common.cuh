@@ -58,36 +58,6 @@ __device__ __forceinline__ uint32_t lower_bound32(const uint32_t *__restrict__ a
 	return lo;
 }
 
-// Lower bound with four-way steps while the range holds more than 32
-// entries: three independent probes per dependent load round trip, so the
-// range shrinks fourfold per trip instead of twofold; then halving over the
-// last (at most 32) entries, one or two 128-byte lines.
-__device__ __forceinline__ uint32_t lower_bound32_w4(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi,
-													 uint32_t x)
-{
-	while (hi - lo > 32)
-	{
-		const uint32_t q = (hi - lo) >> 2;
-		const uint32_t p1 = lo + q, p2 = p1 + q, p3 = p2 + q;
-		const uint32_t v1 = __ldg(a + p1), v2 = __ldg(a + p2), v3 = __ldg(a + p3);
-		if (v1 >= x)
-			hi = p1;
-		else if (v2 >= x)
-		{
-			lo = p1 + 1;
-			hi = p2;
-		}
-		else if (v3 >= x)
-		{
-			lo = p2 + 1;
-			hi = p3;
-		}
-		else
-			lo = p3 + 1;
-	}
-	return lower_bound32(a, lo, hi, x);
-}
-
 // Warp-aggregated append: every lane with pred set gets a distinct slot.
 __device__ __forceinline__ uint32_t warp_append(bool pred, uint32_t *counter)
 {

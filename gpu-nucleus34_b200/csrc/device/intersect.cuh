@@ -131,8 +131,6 @@ __device__ __forceinline__ WarpSample warp_sample(const uint32_t *__restrict__ a
 
 // Lower bounds in [lo, hi) using a sample taken over [lo0, hi) with lo0 <= lo
 // (every entry before lo is below every x searched now). Called by all lanes.
-// W4: the per-lane search within the sample slice takes four-way steps.
-template <bool W4 = false>
 __device__ __forceinline__ uint32_t sampled_lower_bound(const uint32_t *__restrict__ a, const WarpSample &s,
 														uint32_t lo, uint32_t hi, bool want, uint32_t x)
 {
@@ -165,7 +163,7 @@ __device__ __forceinline__ uint32_t sampled_lower_bound(const uint32_t *__restri
 	}
 	uint32_t r = hi;
 	if (want)
-		r = W4 ? lower_bound32_w4(a, l, h, x) : lower_bound32(a, l, h, x);
+		r = lower_bound32(a, l, h, x);
 	return r;
 }
 

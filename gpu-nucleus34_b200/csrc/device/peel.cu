@@ -746,7 +746,7 @@ struct DebitSmem
 // 32 live cliques instead of once per merge step that has any. Next-frontier
 // appends go to the list Fn (or bitmap Bn with BITS). COH: the flags are read
 // through L2 (a kernel that wrote them earlier in the same launch).
-template <bool BITS, bool COH, bool W4 = false>
+template <bool BITS, bool COH>
 __device__ __forceinline__ void debit_warp_tri(uint32_t t, const Lists &L, const DebitSmem &sm, CtlX *ctl,
 											   uint32_t *__restrict__ Fn, uint32_t *__restrict__ Bn,
 											   const uint32_t *__restrict__ third, const uint32_t *itri,
@@ -834,7 +834,7 @@ __device__ __forceinline__ void debit_warp_tri(uint32_t t, const Lists &L, const
 		else
 #endif
 		{
-			pc = sampled_lower_bound<W4>(third, cs, lo_c, L.c1, v, x);
+			pc = sampled_lower_bound(third, cs, lo_c, L.c1, v, x);
 			if (v && pc < L.c1)
 			{
 				xc = __ldg(third + pc);
@@ -998,7 +998,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 
 // The pipelined instantiation returns before the generic walk below.
 #pragma nv_diag_suppress 128
-template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false, bool PIPE = false, bool W4 = false>
+template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false, bool PIPE = false>
 __global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
 	uint32_t *__restrict__ B1, uint64_t W, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
@@ -1170,7 +1170,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : N34_DEBIT_MINB) k_deb
 		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 <= LANE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
-		debit_warp_tri<BITS, false, W4>(t, L, sm, ctl, Fn, Bn, third, itri, S, level, T);
+		debit_warp_tri<BITS, false>(t, L, sm, ctl, Fn, Bn, third, itri, S, level, T);
 	}
 }
 #pragma nv_diag_default 128
@@ -1728,7 +1728,7 @@ __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 template <uint32_t LM>
 void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool lean, CtlX *ctl, const Frontier &fr,
 						const uint32_t *tris, const Incidence &inc, int32_t *S, uint64_t T, cudaEvent_t ev5,
-						bool chunked, bool pipelined, bool wide4)
+						bool chunked, bool pipelined)
 {
 	k_debit_flags_thread<LM><<<gscan, PEEL_THREADS, 0, st>>>(ctl, fr, tris, inc.span, inc.third, inc.tri, S, T,
 															 chunked);
@@ -1759,9 +1759,6 @@ void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool le
 																			tris, inc.span, inc.third, inc.tri, S, T);
 	else if (pipelined)
 		k_debit_flags_warp<false, LM, false, true><<<gwarp, PEEL_THREADS, 0, st>>>(
-			ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris, inc.span, inc.third, inc.tri, S, T);
-	else if (wide4)
-		k_debit_flags_warp<false, LM, false, false, true><<<gwarp, PEEL_THREADS, 0, st>>>(
 			ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris, inc.span, inc.third, inc.tri, S, T);
 	else
 		k_debit_flags_warp<false, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
@@ -1842,8 +1839,6 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 	const bool chunked = !lean && (c.opt_flags & NUCLEUS34_OPT_CHUNKED_DEBIT);
 	// software-pipelined warp debit (list frontiers) when asked for
 	const bool pipelined = !lean && !chunked && (c.opt_flags & NUCLEUS34_OPT_PIPELINED_DEBIT);
-	// four-way searches for the warp debit's lookups on the longest list
-	const bool wide4 = !lean && !chunked && !pipelined && (c.opt_flags & NUCLEUS34_OPT_DEBIT_WIDE_SEARCH);
 	const bool k_in_s = (K == S);
 	int32_t *Kw = k_in_s ? nullptr : K;
 	const uint64_t fwords = (T + 31) / 32;
@@ -2001,13 +1996,13 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				static_assert(THREAD_MODE_MAX == TUNE_LANE_MAX, "default lane/warp split");
 				if (tn.lane_max == 8)
 					launch_debit_flags<8>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked,
-											pipelined, wide4);
+											pipelined);
 				else if (tn.lane_max == 32)
 					launch_debit_flags<32>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked,
-											pipelined, wide4);
+											pipelined);
 				else
 					launch_debit_flags<THREAD_MODE_MAX>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T,
-														ev5, chunked, pipelined, wide4);
+														ev5, chunked, pipelined);
 				tick(6);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, c.dsrc, c.dE, inc.span,
 																	   inc.third, inc.tpos, inc.tri, 3 * T);

@@ -424,7 +424,6 @@ OPT_FRONTIER_BY_C = 0x80
 OPT_CHUNKED_DEBIT = 0x100
 OPT_SCALAR_SCANS = 0x200
 OPT_PIPELINED_DEBIT = 0x400
-OPT_DEBIT_WIDE_SEARCH = 0x1000
 
 
 # The tune table the autotuner wrote on a B200 for this build's measured graph

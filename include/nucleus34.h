@@ -132,10 +132,6 @@ typedef struct
  * triangles' ids and records before the current one's debit (a software
  * pipeline; 5 instead of 6 blocks per SM). Results are identical. */
 #define NUCLEUS34_OPT_PIPELINED_DEBIT 0x400u
-/* opts.flags: the warp debit's lookups on the longest list search with
- * three probes per step (four-way) instead of halving. Results are
- * identical. */
-#define NUCLEUS34_OPT_DEBIT_WIDE_SEARCH 0x1000u
 
 typedef struct
 {
