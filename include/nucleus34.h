@@ -387,7 +387,7 @@ typedef struct
 	uint32_t workers;             /* concurrent passes per device, 0 = 3 */
 	uint64_t max_batch_graphs;    /* requests per pass, 0 = 256 */
 	uint32_t route;               /* NUCLEUS34_ROUTE_* */
-	uint32_t direct_div;          /* ROUTE_MEMORY: direct estimate <= budget / direct_div; 0 = default */
+	uint32_t direct_div;          /* ROUTE_MEMORY: direct estimate <= budget / direct_div; 0 = 64 */
 	uint32_t device_count;        /* 0: opts.device alone; else devices[0..device_count) */
 	const int *devices;           /* ordinals (one may repeat: several budgets on one GPU) */
 	uint32_t concurrent_runs;     /* decompositions running at once per slot (the other workers
