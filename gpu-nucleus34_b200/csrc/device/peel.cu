@@ -43,11 +43,6 @@ constexpr int PEEL_THREADS = 256;
 // call returns NUCLEUS34_E_TIMEOUT: a bound on a loop that would otherwise
 // only end by the round bound. R-MAT scale 20 peels in about 2 s.
 constexpr unsigned long long PEEL_TIME_LIMIT_NS = 600ull * 1000000000ull;
-// Warp debit on one wave of blocks that claim frontier entries from an
-// atomic cursor (build option; off: a static warp stride over 2.7 waves).
-#ifndef N34_DEBIT_CURSOR
-#define N34_DEBIT_CURSOR 0
-#endif
 
 struct CtlX
 {
@@ -67,9 +62,7 @@ struct CtlX
 	// profiling counters of k_debit_flags_warp (filled only when stats is set)
 	uint32_t stats;
 	unsigned long long st_tri, st_merge_entries, st_steps, st_lookups, st_resolves, st_staged, st_found;
-#if N34_DEBIT_CURSOR
-	uint32_t cursor; // next unclaimed frontier position / bitmap word of the warp debit
-#endif
+	uint32_t cursor; // next unclaimed frontier position / bitmap word (warp debit with a cursor)
 };
 
 // A frontier is a list F[0, nF) (default) or, in the memory-lean peel, a
@@ -142,9 +135,7 @@ __global__ void k_peel_init(int32_t *__restrict__ K, uint64_t T, CtlX *ctl, uint
 		ctl->compact_now = 0;
 		ctl->compact_div = compact_div;
 		ctl->sort_min = sort_min;
-#if N34_DEBIT_CURSOR
 		ctl->cursor = 0;
-#endif
 		ctl->peeled_at_compact = 0;
 		ctl->live_at_compact = T;
 		unsigned long long now;
@@ -710,7 +701,6 @@ __device__ __forceinline__ void settle_flags(uint32_t t, uint32_t q0, uint32_t q
 #ifndef N34_DEBIT_MINB
 #define N34_DEBIT_MINB 6
 #endif
-#if N34_DEBIT_CURSOR
 // Claims the next `claim` positions below cap from *cursor into [cpos, cend);
 // false when none are left. Called by all lanes with warp-uniform values.
 // Positions are 32-bit: the death-flag peel has T <= 2^30, and the cursor
@@ -728,7 +718,6 @@ __device__ __forceinline__ bool claim_range(uint32_t *cursor, uint32_t claim, ui
 	cend = cap - b > claim ? b + claim : cap;
 	return true;
 }
-#endif
 
 // Shared memory of one warp of the warp debit: the queue of lookups on the
 // longest list, and a copy of that list's thirds when it is short.
@@ -998,7 +987,7 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 
 // The pipelined instantiation returns before the generic walk below.
 #pragma nv_diag_suppress 128
-template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false, bool PIPE = false>
+template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false, bool PIPE = false, bool CURSOR = false>
 __global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : N34_DEBIT_MINB) k_debit_flags_warp(
 	CtlX *ctl, uint32_t *__restrict__ F0, uint32_t *__restrict__ F1, uint32_t *__restrict__ B0,
 	uint32_t *__restrict__ B1, uint64_t W, const uint32_t *__restrict__ tris, const uint2 *__restrict__ span,
@@ -1105,18 +1094,19 @@ __global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : N34_DEBIT_MINB) k_deb
 		}
 		return;
 	}
-#if N34_DEBIT_CURSOR
-	// [cpos, cend): frontier positions (list) or bitmap words claimed by this
-	// warp; a claim takes CLAIM of them from the round's cursor (warp-uniform)
+	// The warp's next triangle comes either from the positions (list) or
+	// bitmap words it claims, CLAIM at a time, from the round's cursor (CURSOR:
+	// one wave of blocks, balanced at run time), or from a fixed warp stride
+	// over the frontier. [cpos, cend): the current claim; fi: the stride's
+	// position (list) or bitmap word, advanced by each branch itself.
 	constexpr uint32_t CLAIM = BITS ? 4 : 16;
 	const uint32_t cap = BITS ? uint32_t(W) : nF;
 	uint32_t cpos = 0, cend = 0;
-	(void)warp;
-	(void)nwarps;
+	uint64_t fi = warp;
 	for (;;)
 	{
 		uint32_t t;
-		if (BITS)
+		if (CURSOR && BITS)
 		{
 			// next nonzero word of the claim, claiming again when it is used up
 			while (!word)
@@ -1134,18 +1124,13 @@ __global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : N34_DEBIT_MINB) k_deb
 			if (!word)
 				++cpos;
 		}
-		else
+		else if (CURSOR)
 		{
 			if (cpos >= cend && !claim_range(&ctl->cursor, CLAIM, cap, cpos, cend))
 				break;
 			t = F[cpos++];
 		}
-#else
-	// fi: list position, or bitmap word, advanced by the bitmap branch itself
-	for (uint64_t fi = warp;; fi += (BITS ? 0 : nwarps))
-	{
-		uint32_t t;
-		if (BITS)
+		else if (BITS)
 		{
 			while (!word && fi < W)
 			{
@@ -1165,8 +1150,8 @@ __global__ void __launch_bounds__(PEEL_THREADS, PIPE ? 5 : N34_DEBIT_MINB) k_deb
 			if (fi >= nF)
 				break;
 			t = F[fi];
+			fi += nwarps;
 		}
-#endif
 		const Lists L = frontier_lists(t, tris, span);
 		if (L.a1 - L.a0 <= LANE_MAX)
 			continue; // the thread kernel took it (warp-uniform)
@@ -1447,9 +1432,7 @@ __global__ void k_advance(CtlX *ctl)
 	c.nNext = 0;
 	c.minS = INF;
 	ctl->scan = c.nF == 0;
-#if N34_DEBIT_CURSOR
 	ctl->cursor = 0;
-#endif
 }
 
 // ---- small rounds in one cooperative launch ----------------------------------
@@ -1648,9 +1631,7 @@ __global__ void __launch_bounds__(PEEL_THREADS, 4) k_small_rounds(
 			c.minS = INF;
 			ctl->scan = nNext == 0;
 			ctl->small_rounds++;
-#if N34_DEBIT_CURSOR
 			ctl->cursor = 0;
-#endif
 		}
 		if (!grid_barrier(bar, gen, deadline))
 		{
@@ -1728,21 +1709,22 @@ __global__ void k_stats(CtlX *ctl, const int32_t *__restrict__ K, uint64_t T)
 template <uint32_t LM>
 void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool lean, CtlX *ctl, const Frontier &fr,
 						const uint32_t *tris, const Incidence &inc, int32_t *S, uint64_t T, cudaEvent_t ev5,
-						bool chunked, bool pipelined)
+						bool chunked, bool pipelined, bool cursor)
 {
 	k_debit_flags_thread<LM><<<gscan, PEEL_THREADS, 0, st>>>(ctl, fr, tris, inc.span, inc.third, inc.tri, S, T,
 															 chunked);
 	if (ev5)
 		cudaEventRecord(ev5, st);
-#if N34_DEBIT_CURSOR
+	if (cursor)
 	{
 		// one wave: as many blocks as can be resident at once on every SM
 		int dev = 0, sms = 1, per_sm = 1;
 		if (cudaGetDevice(&dev) != cudaSuccess ||
 			cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-			cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-				&per_sm, lean ? k_debit_flags_warp<true, LM> : k_debit_flags_warp<false, LM>, PEEL_THREADS, 0) !=
-				cudaSuccess ||
+			cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm,
+														  lean ? k_debit_flags_warp<true, LM, false, false, true>
+															   : k_debit_flags_warp<false, LM, false, false, true>,
+														  PEEL_THREADS, 0) != cudaSuccess ||
 			per_sm < 1)
 		{
 			cudaGetLastError();
@@ -1750,8 +1732,10 @@ void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool le
 		}
 		gwarp = uint32_t(per_sm) * uint32_t(sms > 0 ? sms : 1);
 	}
-#endif
-	if (lean)
+	if (lean && cursor)
+		k_debit_flags_warp<true, LM, false, false, true><<<gwarp, PEEL_THREADS, 0, st>>>(
+			ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris, inc.span, inc.third, inc.tri, S, T);
+	else if (lean)
 		k_debit_flags_warp<true, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
 																	 inc.span, inc.third, inc.tri, S, T);
 	else if (chunked)
@@ -1759,6 +1743,9 @@ void launch_debit_flags(cudaStream_t st, uint32_t gscan, uint32_t gwarp, bool le
 																			tris, inc.span, inc.third, inc.tri, S, T);
 	else if (pipelined)
 		k_debit_flags_warp<false, LM, false, true><<<gwarp, PEEL_THREADS, 0, st>>>(
+			ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris, inc.span, inc.third, inc.tri, S, T);
+	else if (cursor)
+		k_debit_flags_warp<false, LM, false, false, true><<<gwarp, PEEL_THREADS, 0, st>>>(
 			ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris, inc.span, inc.third, inc.tri, S, T);
 	else
 		k_debit_flags_warp<false, LM><<<gwarp, PEEL_THREADS, 0, st>>>(ctl, fr.F0, fr.F1, fr.B0, fr.B1, fr.W, tris,
@@ -1839,6 +1826,8 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 	const bool chunked = !lean && (c.opt_flags & NUCLEUS34_OPT_CHUNKED_DEBIT);
 	// software-pipelined warp debit (list frontiers) when asked for
 	const bool pipelined = !lean && !chunked && (c.opt_flags & NUCLEUS34_OPT_PIPELINED_DEBIT);
+	// warp debit on one wave that claims frontier positions from a cursor
+	const bool cursor = !chunked && !pipelined && (c.opt_flags & NUCLEUS34_OPT_DEBIT_CURSOR);
 	const bool k_in_s = (K == S);
 	int32_t *Kw = k_in_s ? nullptr : K;
 	const uint64_t fwords = (T + 31) / 32;
@@ -1996,13 +1985,13 @@ int peel(Ctx &c, int variant, const Incidence &inc, const CliqueCsr &csr, int32_
 				static_assert(THREAD_MODE_MAX == TUNE_LANE_MAX, "default lane/warp split");
 				if (tn.lane_max == 8)
 					launch_debit_flags<8>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked,
-											pipelined);
+											pipelined, cursor);
 				else if (tn.lane_max == 32)
 					launch_debit_flags<32>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T, ev5, chunked,
-											pipelined);
+											pipelined, cursor);
 				else
 					launch_debit_flags<THREAD_MODE_MAX>(c.stream, gscan, gwarp, lean, ctl, fr, c.dtris, inc, S, T,
-														ev5, chunked, pipelined);
+														ev5, chunked, pipelined, cursor);
 				tick(6);
 				k_finalize_flags<<<gscan, PEEL_THREADS, 0, c.stream>>>(ctl, fr, c.dtris, c.dsrc, c.dE, inc.span,
 																	   inc.third, inc.tpos, inc.tri, 3 * T);

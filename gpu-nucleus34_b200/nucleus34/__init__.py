@@ -424,6 +424,7 @@ OPT_FRONTIER_BY_C = 0x80
 OPT_CHUNKED_DEBIT = 0x100
 OPT_SCALAR_SCANS = 0x200
 OPT_PIPELINED_DEBIT = 0x400
+OPT_DEBIT_CURSOR = 0x800
 
 
 # The tune table the autotuner wrote on a B200 for this build's measured graph

@@ -132,6 +132,11 @@ typedef struct
  * triangles' ids and records before the current one's debit (a software
  * pipeline; 5 instead of 6 blocks per SM). Results are identical. */
 #define NUCLEUS34_OPT_PIPELINED_DEBIT 0x400u
+/* opts.flags: the warp debit of the death-flag peel runs as one wave of
+ * blocks whose warps claim frontier positions from an atomic cursor (work
+ * balanced at run time) instead of a fixed warp stride. Results are
+ * identical. */
+#define NUCLEUS34_OPT_DEBIT_CURSOR 0x800u
 
 typedef struct
 {

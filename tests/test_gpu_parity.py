@@ -213,7 +213,7 @@ def test_chunked_debit_schedule_matches(n34, oracle, case):
 @pytest.mark.parametrize("case", [("rmat", 13, 16, 3), ("rgg", 30000, 40, 9)])
 def test_scan_and_pipeline_options_match(n34, oracle, case):
     """The level-change scans (vectorised or one word per thread) and the warp
-    debit (plain or software-pipelined) give the
+    debit (static stride, software-pipelined, or claimed from a cursor) give the
     oracle's k, with list frontiers and with the bitmap frontiers of the lean
     layout."""
     if case[0] == "rmat":
@@ -226,6 +226,9 @@ def test_scan_and_pipeline_options_match(n34, oracle, case):
         n34.OPT_SCALAR_SCANS,
         n34.OPT_PIPELINED_DEBIT,
         n34.OPT_PIPELINED_DEBIT | n34.OPT_NO_SMALL_ROUNDS,
+        n34.OPT_DEBIT_CURSOR,
+        n34.OPT_DEBIT_CURSOR | n34.OPT_NO_SMALL_ROUNDS,
+        n34.OPT_DEBIT_CURSOR | n34.OPT_LEAN_MEMORY,
         n34.OPT_LEAN_MEMORY,
         n34.OPT_LEAN_MEMORY | n34.OPT_SCALAR_SCANS,
         n34.OPT_NO_SMALL_ROUNDS | n34.OPT_SCALAR_SCANS,
