@@ -27,6 +27,7 @@
 //
 // Results do not depend on the mix: a graph's triangles, cliques and k in a
 // union equal those of the graph alone (the batched form's argument).
+#include "admission.h"
 #include "pipeline.cuh"
 
 #include <algorithm>
@@ -74,21 +75,8 @@ struct Request
 	uint64_t pass = 0; // pass that served it
 };
 
-// Bytes of one pass per triangle (peak: listing, incidence build, support,
-// peel arrays) and per oriented edge (CSR, sources, spans, counts); the
-// direct variant adds its clique list and triangle->clique incidence (16 +
-// 16 bytes per clique) and one destroyed flag per clique. Applied to the
-// out-wedge and out-triple bounds, not to the true counts, so they
-// overestimate; tests/test_server.py checks them against measured peaks.
-constexpr uint64_t PASS_BYTES_PER_TRIANGLE = 80;
-constexpr uint64_t PASS_BYTES_PER_EDGE = 40;
-constexpr uint64_t DIRECT_BYTES_PER_CLIQUE = 33;
-// Direct share of a slot's budget (1/64). Alone, a graph is decomposed
-// faster by the direct variant up to about 1e8 four-cliques, but a direct
-// union of many such graphs streams its clique list from DRAM where the
-// graph alone kept it in L2: on the full serving mix (edges up to 1e7) a
-// share of 1/8 served 13.3-13.7 graphs/s, 1/64 14.2 and on-demand only 14.3.
-constexpr uint32_t DEFAULT_DIRECT_DIV = 64;
+// The admission constants (bytes per triangle, edge and clique bound) and
+// the default direct share live with the estimates in admission.h.
 
 struct Slot
 {
@@ -120,22 +108,6 @@ struct nucleus34_server_s
 };
 
 namespace {
-
-// Out-wedges sum_u C(d, 2) (bound on the triangles) and out-triples
-// sum_u C(d, 3) (bound on the four-cliques); the triples saturate at 2^63.
-void out_bounds(const uint32_t *D, uint64_t n, uint64_t &wedges, uint64_t &triples)
-{
-	wedges = 0;
-	triples = 0;
-	for (uint64_t u = 0; u < n; ++u)
-	{
-		const uint64_t d = D[u];
-		wedges += d * (d ? d - 1 : 0) / 2;
-		const unsigned __int128 t3 = d >= 3 ? (unsigned __int128)d * (d - 1) * (d - 2) / 6 : 0;
-		const unsigned __int128 sum = (unsigned __int128)triples + t3;
-		triples = sum > ((unsigned __int128)1 << 63) ? (uint64_t(1) << 63) : uint64_t(sum);
-	}
-}
 
 // Entry to and exit from a slot's decompositions (at most max_running at
 // once when set). The union build, upload and result copies stay outside, so
@@ -427,22 +399,16 @@ int nucleus34_server_submit(nucleus34_server s, const nucleus34_csr *csr, uint32
 	if (acc != csr->m)
 		return fail(NUCLEUS34_E_INVALID, "sum of D does not equal m");
 	q->O[csr->n] = uint32_t(acc);
-	uint64_t w = 0, t3 = 0;
-	out_bounds(csr->D, csr->n, w, t3);
-	q->est_triangles = w;
-	q->est_cliques = t3;
-	const uint64_t est_on = PASS_BYTES_PER_EDGE * csr->m + PASS_BYTES_PER_TRIANGLE * w;
-	const unsigned __int128 est_dir128 = (unsigned __int128)est_on + (unsigned __int128)DIRECT_BYTES_PER_CLIQUE * t3;
-	const uint64_t est_dir = est_dir128 > ~uint64_t(0) ? ~uint64_t(0) : uint64_t(est_dir128);
 	// routing by the memory estimate (the smallest slot budget is the limit)
 	uint64_t min_budget = ~uint64_t(0);
 	for (auto &sl : s->slots)
 		min_budget = std::min(min_budget, sl.budget);
-	if (flags & NUCLEUS34_REQ_CLIQUES)
-		q->direct = true;
-	else if (s->route == NUCLEUS34_ROUTE_MEMORY)
-		q->direct = est_dir <= min_budget / s->direct_div && t3 < 0xffffffffull;
-	q->est_bytes = q->direct ? est_dir : est_on;
+	nucleus34_request_estimate est{};
+	request_estimate(csr->D, csr->n, csr->m, min_budget, s->route, s->direct_div, flags, est);
+	q->est_triangles = est.triangle_bound;
+	q->est_cliques = est.clique_bound;
+	q->direct = est.direct != 0;
+	q->est_bytes = q->direct ? est.direct_bytes : est.ondemand_bytes;
 	q->t_submit = clk::now();
 	{
 		std::lock_guard<std::mutex> lk(s->mu);

@@ -57,7 +57,7 @@ EXPORTED = (
     "nucleus34_graph_release", "nucleus34_graph_csr",
     "nucleus34_gen_rmat", "nucleus34_gen_rgg", "nucleus34_gen_ws",
     "nucleus34_edges_write", "nucleus34_edges_release", "nucleus34_splitmix64",
-    "nucleus34_graph_cost", "nucleus34_split_plan",
+    "nucleus34_graph_cost", "nucleus34_split_plan", "nucleus34_server_estimate",
 )
 
 
@@ -148,6 +148,11 @@ class RequestInfo(C.Structure):
                 "latency_seconds": self.latency_seconds, "pass": self.pass_, "direct": bool(self.direct)}
 
 
+class RequestEstimate(C.Structure):
+    _fields_ = [("ondemand_bytes", C.c_uint64), ("direct_bytes", C.c_uint64), ("triangle_bound", C.c_uint64),
+                ("clique_bound", C.c_uint64), ("direct", C.c_int)]
+
+
 class ServerCounters(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("passes", "served", "pending", "busy_workers", "workers",
                                           "in_flight_bytes", "budget_bytes", "direct_served", "devices")]
@@ -211,6 +216,9 @@ def lib() -> C.CDLL:
     L.nucleus34_split_plan.argtypes = [C.POINTER(C.c_uint64), C.c_uint64, C.c_uint32, C.POINTER(C.c_uint32),
                                        C.POINTER(C.c_uint64)]
     L.nucleus34_split_plan.restype = C.c_int
+    L.nucleus34_server_estimate.argtypes = [C.POINTER(Csr), C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                                            C.POINTER(RequestEstimate)]
+    L.nucleus34_server_estimate.restype = C.c_int
     L.nucleus34_server_create.argtypes = [C.POINTER(Opts), C.POINTER(ServerOpts), C.POINTER(C.c_void_p)]
     L.nucleus34_server_create.restype = C.c_int
     L.nucleus34_server_submit.argtypes = [C.c_void_p, C.POINTER(Csr), C.c_uint32, C.POINTER(C.c_uint64)]
@@ -322,6 +330,21 @@ def split_plan(costs, parts: int):
                                       _u32p(part_of) if len(c) else None,
                                       load.ctypes.data_as(C.POINTER(C.c_uint64))), "split_plan")
     return part_of, load[:parts]
+
+
+def server_estimate(g: "HostGraph", budget: int, route: int = 0, direct_div: int = 0,
+                    cliques: bool = False, triangles: bool = False) -> dict:
+    """The serving loop's admission estimates and variant for g, without a
+    server or a device (nucleus34_server_estimate): budget is the smallest
+    slot budget, route a ROUTE_* constant, direct_div 0 for the default."""
+    e = RequestEstimate()
+    csr = g.csr()
+    flags = (REQ_CLIQUES if cliques else 0) | (REQ_TRIANGLES if triangles else 0)
+    _check(lib().nucleus34_server_estimate(C.byref(csr), budget, route, direct_div, flags, C.byref(e)),
+           "server_estimate")
+    return {"ondemand_bytes": int(e.ondemand_bytes), "direct_bytes": int(e.direct_bytes),
+            "triangle_bound": int(e.triangle_bound), "clique_bound": int(e.clique_bound),
+            "direct": bool(e.direct)}
 
 
 @dataclass

@@ -416,6 +416,24 @@ typedef struct
 	uint64_t devices;             /* device slots */
 } nucleus34_server_counters;
 
+/* A request's admission estimates and variant, as nucleus34_server_submit
+ * computes them (host only; needs no device). */
+typedef struct
+{
+	uint64_t ondemand_bytes;      /* pass memory estimate of the on-demand variant */
+	uint64_t direct_bytes;        /* the same with the direct variant's clique list (saturates) */
+	uint64_t triangle_bound;      /* out-wedges sum_u C(d+(u), 2) >= triangles */
+	uint64_t clique_bound;        /* out-triples sum_u C(d+(u), 3) >= four-cliques (saturates at 2^63) */
+	int direct;                   /* 1 if the request would be routed to the direct variant */
+} nucleus34_request_estimate;
+
+/* Estimates and routes a request without submitting it: budget is the
+ * smallest slot budget the server would see, route and direct_div as in
+ * nucleus34_server_opts (direct_div 0 = 64), flags as in submit. Reads only
+ * csr->D (sum must equal m). No reference counterpart. */
+int nucleus34_server_estimate(const nucleus34_csr *csr, uint64_t budget, uint32_t route, uint32_t direct_div,
+                              uint32_t flags, nucleus34_request_estimate *out);
+
 int nucleus34_server_create(const nucleus34_opts *opts, const nucleus34_server_opts *sopts, nucleus34_server *out);
 /* Copies the CSR and queues it; returns at once with the request id. */
 int nucleus34_server_submit(nucleus34_server s, const nucleus34_csr *csr, uint32_t flags, uint64_t *id);
