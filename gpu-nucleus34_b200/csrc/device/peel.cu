@@ -985,6 +985,14 @@ __global__ void __launch_bounds__(PEEL_THREADS) k_debit_flags_thread(
 	});
 }
 
+// Debit of the round's dying triangles whose shortest list is longer than
+// LANE_MAX, one warp per triangle (shorter ones: k_debit_flags_thread).
+// BITS: bitmap frontiers (memory-lean layout) instead of lists. The other
+// parameters choose how warps walk a list frontier; all give the same k:
+// CHUNKED, a warp loads up to 32 triangles' records at once and its lanes
+// also debit the short lists; PIPE, the next triangles' ids and records are
+// loaded ahead of the current debit; CURSOR, one wave of blocks claims
+// positions from an atomic cursor. Default: a fixed warp stride.
 // The pipelined instantiation returns before the generic walk below.
 #pragma nv_diag_suppress 128
 template <bool BITS, uint32_t LANE_MAX, bool CHUNKED = false, bool PIPE = false, bool CURSOR = false>
